@@ -1,0 +1,416 @@
+"""Benchmark: the fused radix partition -> unique-build hash join -> dense
+group-by of the 150M-row build x 600M-row probe workload on one B200
+(SELECT group, SUM(price*(100-disc)), COUNT(*) ... GROUP BY group over 1.5M
+groups), reported as join+agg rows/s = (build rows + probe rows) / s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step is one full pass over resident inputs: partition both sides, build
+and probe every round, aggregate, and compact the occupied groups (one host
+wait for the bucket counts, one for the group count).  Under torchrun each
+rank runs an independent replica of the workload on its own GPU (the path is
+replicas-only across GPUs); the time is the max over ranks.
+
+The JSON line also carries: the dominant kernel's live roofline (algorithmic
+bytes per launch / CUDA-event launch time, against the measured HBM copy
+bandwidth), the whole step's, the end-to-end rate through the public API with
+host buffers and host<->device copies inside the timed region, the oracle's
+CPU rate on a bounded sample, the SM clocks sampled during the timed region,
+and the number of this library's kernels launched in it.  ``--impl
+reference`` times the reference algorithm's CPU restatement (the oracle) on
+all host threads instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="scale",
+                    help="scale (150M x 600M), small (250K x 1M) or scale/<divisor>")
+    ap.add_argument("--B", type=int, default=0, help="fan-out (0: the autotuner's pick)")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", type=float, default=0.01,
+                    help="fraction of the workload the CPU baseline joins per sample")
+    return ap.parse_args(argv)
+
+
+def workload(name: str):
+    from pageflow_b200 import datagen
+    if name == "scale":
+        return datagen.SCALE
+    if name == "small":
+        return datagen.SMALL
+    if name.startswith("scale/"):
+        return datagen.scaled(datagen.SCALE, 1 / float(name.split("/", 1)[1]))
+    raise SystemExit(f"unknown workload {name}")
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---- clocks -------------------------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi samples of this GPU's clocks every 100 ms while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str | None):
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        cmd = ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+               "-lms", "100"]
+        if gpu_id:
+            cmd += ["-i", gpu_id]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        rows = []
+        for line in Path(self.file.name).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in rows if num(r[2]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4)
+                          if r[5 + i].lower() in ("active", "1", "yes")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ---- the reference arm / CPU baseline -------------------------------------------
+
+def cpu_sample_run(w, frac: float, reps_seconds: float = 10.0):
+    """The oracle's join + group-by (the reference algorithm restated in C,
+    partitioned by mix64 and joined by sort + binary search on every host
+    thread) on a bounded sample of the workload: `frac` of its rows, repeated
+    for about `reps_seconds`.  Returns (rows/s, threads, description)."""
+    import oracle
+    oracle.build()
+    nb = max(1, int(w.n_build * frac))
+    npr = max(1, int(w.n_probe * frac))
+    ng = max(1, int(w.n_groups * frac))
+    bkey, bgrp = oracle.gen_build(w.seed, nb, ng)
+    fk, price, disc = oracle.gen_probe(w.config, w.seed, nb, 0, npr)
+    threads = oracle.threads()
+    runs, t0 = 0, time.perf_counter()
+    while True:
+        oracle.join_aggregate(bkey, bgrp, fk, price, disc, w.scale, 0, ng, B=256,
+                              n_threads=threads)
+        runs += 1
+        el = time.perf_counter() - t0
+        if el >= reps_seconds or runs >= 50:
+            break
+    rate = (nb + npr) * runs / el
+    desc = (f"{nb} build x {npr} probe rows ({frac:g} of the workload, {ng} groups), "
+            f"{runs} runs in {el:.1f} s")
+    return rate, threads, desc
+
+
+def run_reference(args, w, world, rank):
+    if rank != 0:
+        return
+    import oracle
+    oracle.build()
+    frac = args.cpu_sample
+    nb = max(1, int(w.n_build * frac))
+    npr = max(1, int(w.n_probe * frac))
+    ng = max(1, int(w.n_groups * frac))
+    bkey, bgrp = oracle.gen_build(w.seed, nb, ng)
+    fk, price, disc = oracle.gen_probe(w.config, w.seed, nb, 0, npr)
+    threads = oracle.threads()
+    for _ in range(args.warmup):
+        oracle.join_aggregate(bkey, bgrp, fk, price, disc, w.scale, 0, ng, B=256,
+                              n_threads=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle.join_aggregate(bkey, bgrp, fk, price, disc, w.scale, 0, ng, B=256,
+                              n_threads=threads)
+    el = time.perf_counter() - t0
+    rate = (nb + npr) * args.steps / el
+    sample = (f"{nb} build x {npr} probe rows per step ({frac:g} of the workload, {ng} "
+              f"groups)")
+    line = {
+        "impl": "reference", "metric": "join+agg rows/s", "value": rate, "unit": "rows/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": w.name, "build_rows": w.n_build, "probe_rows": w.n_probe,
+                   "groups": w.n_groups, "parallelism": "replicas"},
+        "cpu_baseline": {"value": rate, "unit": "rows/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": rate, "unit": "rows/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---- ours ------------------------------------------------------------------------------
+
+def algorithmic_bytes(w, B_rounds):
+    """Algorithmic DRAM bytes per step, per kernel (name -> bytes): the
+    columns each pass must read and write once.  k_fhist reads each side's
+    keys; the scatters read the source columns and write the carried ones
+    (build: key 8 + group 4; probe: fk 8 + value 8, from fk, price and
+    discount); the build and probe rounds read the partitioned sides once;
+    the finish reads the 16-byte slab and writes the groups it keeps."""
+    nb, npr, g = w.n_build, w.n_probe, w.n_groups
+    return {
+        "k_fhist": 8 * (nb + npr),
+        "k_fscatter_build": nb * (12 + 12),
+        "k_fscatter_probe": npr * (24 + 16),
+        "k_fbuild": nb * 12,
+        "k_fprobe": npr * 16,
+        "k_gcount": g * 8,
+        "k_gemit": g * 16 + g * 24,
+    }
+
+
+def run_ours(args, w, world, rank, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    from pageflow_b200 import _native, datagen
+    from pageflow_b200.join_aggregate import JoinAggregate
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    bkey, bgrp = datagen.gen_build(w, dev)
+    fk, price, disc = datagen.gen_probe(w, dev)
+    plan = JoinAggregate(w.n_build, w.n_probe, 0, w.n_groups, dev, B=args.B or None,
+                         scale=w.scale)
+    torch.cuda.synchronize()
+
+    def step():
+        plan.aggregate(bkey, bgrp, fk, price, disc)
+        return plan.finish()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    keys, sums, counts = step()
+    n_groups_out = int(keys.numel())
+    matched = plan.read_stats().matched
+    # rounds of the plan (for the per-launch figures)
+
+    gpu_id = None
+    try:
+        gpu_id = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    sampler = ClockSampler(gpu_id)
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    launches0 = _native.launch_count()
+    _native.profile_begin()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    prof = _native.profile_end()
+    launches = _native.launch_count() - launches0
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    rows_step = w.n_build + w.n_probe
+    value = world * rows_step * args.steps / (ms / 1e3)
+
+    # roofline: the dominant kernel's live figure and the whole step's
+    peak, peak_kind = measured_peak()
+    alg = algorithmic_bytes(w, None)
+    dom = max(prof.items(), key=lambda kv: kv[1][0]) if prof else None
+    roofline = None
+    kernels = {}
+    for name, (tot_ms, n) in sorted(prof.items(), key=lambda kv: -kv[1][0]):
+        per_step_launches = n / args.steps
+        entry = {"ms_per_step": tot_ms / args.steps, "launches_per_step": per_step_launches,
+                 "share": None}
+        if name in alg and tot_ms > 0:
+            entry["gbs"] = alg[name] * args.steps / (tot_ms / 1e3) / 1e9
+        kernels[name] = entry
+    tot_kernel_ms = sum(v[0] for v in prof.values()) or 1.0
+    for name in kernels:
+        kernels[name]["share"] = prof[name][0] / tot_kernel_ms
+    if dom is not None:
+        name, (tot_ms, n) = dom
+        bytes_launch = alg.get(name, 0) * args.steps / n
+        avg_s = tot_ms / n / 1e3
+        achieved = bytes_launch / avg_s / 1e9
+        traffic = None
+        tfile = ROOT / "profiles" / "traffic.json"
+        if tfile.exists():
+            try:
+                tj = json.loads(tfile.read_text())
+                if tj.get("workload") == w.name and name in tj.get("kernels", {}):
+                    traffic = tj["kernels"][name]["dram_bytes_per_launch"]
+            except Exception:
+                traffic = None
+        roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
+                    "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                    "bytes_per_launch": bytes_launch, "peak_source": peak_kind}
+    step_bytes = sum(alg.values())
+    step_gbs = step_bytes / (ms / args.steps / 1e3) / 1e9
+    step_roofline = {"bound": "hbm", "algorithmic_bytes": step_bytes, "achieved": step_gbs,
+                     "peak": peak, "unit": "GB/s", "frac": step_gbs / peak,
+                     "peak_source": peak_kind}
+
+    # end to end through the public API, host buffers
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, w, plan, dev, (bkey, bgrp, fk, price, disc), world)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, threads, desc = cpu_sample_run(w, args.cpu_sample)
+        cpu = {"value": rate, "unit": "rows/s", "cores": threads, "kind": "port",
+               "sample": desc}
+
+    if rank == 0:
+        line = {
+            "metric": "join+agg rows/s", "value": value, "unit": "rows/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int64", "data": "synthetic (seeded generator, inputs on the device)",
+            "config": {"workload": w.name, "build_rows": w.n_build, "probe_rows": w.n_probe,
+                       "groups": w.n_groups, "fanout_B": plan.B, "parallelism":
+                       "replicas" if world > 1 else "single",
+                       "l2": "inputs (16 B/row build, 24 B/row probe) exceed L2; no flush",
+                       "groups_out": n_groups_out, "matched_probe_rows": matched},
+            "roofline": roofline, "step_roofline": step_roofline,
+            "kernels": kernels,
+            "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def run_e2e(args, w, plan, dev, dev_inputs, world):
+    """The same metric with the inputs in pinned host memory: every step
+    copies them to the device, runs the join + group-by and copies the
+    groups back (device-timed, max over ranks)."""
+    import torch
+    import torch.distributed as dist
+    host = [t.cpu().pin_memory() for t in dev_inputs]
+    h2d = sum(t.numel() * t.element_size() for t in host)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        for d, h in zip(dev_inputs, host):
+            d.copy_(h, non_blocking=True)
+        plan.aggregate(*dev_inputs)
+        keys, sums, counts = plan.finish()
+        out = [keys.to("cpu", non_blocking=True), sums.to("cpu", non_blocking=True),
+               counts.to("cpu", non_blocking=True)]
+        return out, sum(x.numel() * 8 for x in (keys, sums, counts))
+
+    step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    d2h = 0
+    for _ in range(args.e2e_steps):
+        _, d2h = step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    value = world * (w.n_build + w.n_probe) * args.e2e_steps / (ms / 1e3)
+    return {"value": value, "unit": "rows/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": ms / args.e2e_steps,
+            "h2d_gbs": h2d / (ms / args.e2e_steps / 1e3) / 1e9}
+
+
+def main(argv=None) -> int:
+    args = parse_args(argv)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    w = workload(args.workload)
+    if args.impl == "reference":
+        run_reference(args, w, world, rank)
+        return 0
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        run_ours(args, w, world, rank, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -1,0 +1,237 @@
+/*
+ * pageflow_b200 — the C ABI of the B200 (sm_100a) relational hot path.
+ *
+ * Every entry point takes plain device pointers, element counts and a
+ * cudaStream_t (passed as void*), returns an int status (PF_OK or a negative
+ * PF_E* code; pf_last_error() gives the message of the calling thread's last
+ * failure) and allocates no device memory: scratch comes from a caller-owned
+ * device workspace whose size the matching *_workspace() function reports.
+ * Outputs are caller-allocated device buffers sized as each function states.
+ * A "host_out" argument is caller-owned PINNED host memory (cudaHostAlloc or
+ * cudaHostRegister) that a kernel writes through its device alias.
+ *
+ * Functions that return a row count to the host wait for it once (a bounded
+ * poll of one CUDA event; PF_ETIMEOUT after pf_set_wait_timeout_ms()); all
+ * other work stays queued on the stream.
+ *
+ * Reference interfaces replaced (PageFlow, operators/kernels/tqpkernels.cu:8-46,
+ * the pybind module TQPlib.tqpkernels):
+ *   pf_partition_sort      <- partition_sort     (operators/kernels/partition_sort.cu:610-768)
+ *   pf_join_unique_hash    <- join_unique_hash   (operators/kernels/join_core.cu:301-351)
+ *   pf_join_semi_anti      <- join_semi_anti     (operators/kernels/join_core.cu:358-400)
+ *   pf_join_expand_prepare
+ *   + pf_join_expand       <- join_expand        (operators/kernels/join_core.cu:263-295)
+ * and the torch tensor programs of the aggregation path:
+ *   pf_slab_add / pf_slab_finish <- DenseAggregationSlab.add/finish (operators/aggregation_slab.py:213-246)
+ *   pf_join_aggregate      <- the partition -> unique-hash join -> index_select ->
+ *                             KeyedAggregate.pass1 -> reduce_tick_slice composition
+ *                             (uvm/join.py:98-225, uvm/aggregate.py:147-212)
+ */
+#ifndef PAGEFLOW_B200_H
+#define PAGEFLOW_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status ------------------------------------------------------------ */
+#define PF_OK 0
+#define PF_EINVAL (-1)   /* an argument outside the function's limits        */
+#define PF_ECUDA (-2)    /* a CUDA runtime call failed                        */
+#define PF_ETIMEOUT (-3) /* a bounded host or device wait gave up             */
+#define PF_ENOSPACE (-4) /* the workspace is smaller than *_workspace() asked */
+#define PF_EDEVICE (-5)  /* a kernel raised its device error word             */
+
+/* The calling thread's last failure message ("" after a success). */
+const char* pf_last_error(void);
+/* Library version, e.g. "0.1.0". */
+const char* pf_version(void);
+/* The bound of every host wait, in milliseconds (default 120000). */
+void pf_set_wait_timeout_ms(int64_t ms);
+/* Kernels this library has launched in the process so far. */
+int64_t pf_launch_count(void);
+/*
+ * Per-kernel timing of the calling thread's launches: between
+ * pf_profile_begin() and pf_profile_end() every launch is bracketed by a pair
+ * of CUDA events on its stream.  pf_profile_end waits for them and fills, for
+ * up to max_kernels distinct kernels, its name (name_len bytes a slot), the
+ * summed milliseconds and the launches; returns the number of distinct
+ * kernels (or a negative PF_E* code).  No counterpart in the reference: it
+ * serves the benchmark's live roofline figures.
+ */
+void pf_profile_begin(void);
+int pf_profile_end(int max_kernels, char* names, int name_len, double* total_ms,
+                   int64_t* launches);
+
+/* ---- limits (kept equal to the reference's) ----------------------------- */
+#define PF_PART_MAX_COLS 6     /* partition_sort.cu:54 MAXC                 */
+#define PF_PART_MAX_WIDTHS 4   /* partition_sort.cu:55 MAXCLS (gidx incl.)  */
+#define PF_PART_B_MAX 512      /* partition_sort.cu:56 BMAX == JOIN_B_MAX   */
+#define PF_JOIN_MAX_ROWS ((int64_t)2147418112) /* join_core.cu:49, 2^31-2^16 */
+
+/* ---- radix partition (drop-in for tqpkernels.partition_sort) ------------ */
+/*
+ * Stable hash partition of up to 6 columns plus the int64 global index into
+ * B padded buckets.  A row's bucket is the top log2(B) bits of mix64(key)
+ * (0 when B == 1); rows keep their domain order inside a bucket; each
+ * non-empty bucket starts on a whole lcm(row_bytes, 512)-byte unit of its
+ * output (rows_per_unit = 512 / gcd(row_bytes, 512)); padding rows are left
+ * unwritten.
+ *
+ *  cols_in[c]    column c: n_dom rows (raw) or n_valid rows (comp[c] = 1,
+ *                already compacted by the mask), row_bytes[c] bytes a row
+ *  cols_out[c]   n_valid + B*(rows_per_unit(row_bytes[c]) - 1) rows
+ *  key_idx       the int64 key column
+ *  mask          NULL, or n_dom bytes (non-zero = kept)
+ *  n_dom         the mask's rows (or the key's rows without a mask), < 2^31
+ *  n_valid       the kept rows (the rows of a compacted column)
+ *  goff          global index of domain row 0; gidx = goff + pre-mask row
+ *  B             power of two in [1, 512]
+ *  select_first  with a mask: collect the kept rows' ids first
+ *  gidx_out      int64, n_valid + B*(rows_per_unit(8) - 1) rows
+ *  host_out      pinned int64[B + 5]: [0,B) bucket counts; [B, B+4) each
+ *                row-width class's padded total (classes numbered by first
+ *                appearance over the columns, then the gidx's 8 B); [B+4] the
+ *                kept rows a mask prologue found, or -1 when none ran.
+ * A kept-row count that the mask contradicts leaves the outputs unwritten
+ * (nothing is read or written past what n_valid sizes); the caller compares
+ * host_out against n_valid.  Waits once, for the counts.
+ */
+size_t pf_partition_sort_workspace(int64_t n_dom, int64_t n_valid, int B, int has_mask,
+                                   int select_first);
+int pf_partition_sort(const void* const* cols_in, void* const* cols_out, const int* row_bytes,
+                      const int* comp, int ncols, int key_idx, const uint8_t* mask, int64_t n_dom,
+                      int64_t n_valid, int64_t goff, int B, int select_first, int64_t* gidx_out,
+                      int64_t* host_out, void* workspace, size_t workspace_bytes, void* stream);
+/* 512 / gcd(row_bytes, 512): rows of one padding unit. */
+int64_t pf_rows_per_unit(int64_t row_bytes);
+
+/* ---- join cores (drop-ins for join_unique_hash / join_semi_anti / join_expand) */
+/*
+ * Inner join on a unique build tuple of 1 or 2 int64 keys.  build_idx and
+ * probe_idx have n_probe rows each; the first host_out[0] hold the matches in
+ * probe-row order.  host_out: pinned int64[2] ([1] is set to 0).  Waits once.
+ * 1 <= n_build, n_probe <= PF_JOIN_MAX_ROWS.
+ */
+size_t pf_join_unique_hash_workspace(int64_t n_build, int64_t n_probe);
+int pf_join_unique_hash(const int64_t* build0, const int64_t* build1, int64_t n_build,
+                        const int64_t* probe0, const int64_t* probe1, int64_t n_probe, int nkeys,
+                        int64_t* build_idx, int64_t* probe_idx, int64_t* host_out,
+                        void* workspace, size_t workspace_bytes, void* stream);
+
+/* Residual operators of a semi/anti summary, as build.v OP probe.v. */
+#define PF_OP_NONE 0
+#define PF_OP_NE 1
+#define PF_OP_LT 2
+#define PF_OP_LE 3
+#define PF_OP_GT 4
+#define PF_OP_GE 5
+/*
+ * Semi (anti = 0) or anti (anti = 1) join on a hash set of build keys; with
+ * op != PF_OP_NONE a match must also pass build_val OP probe_val for some
+ * build row of the key (answered by the key's min and/or max).  out has
+ * n_probe rows; the first host_out[0] are the kept probe rows, ascending.
+ * host_out[1] = 1 when a build key equals INT64_MIN (the empty-slot value;
+ * the result is then not valid).  Waits once.
+ */
+size_t pf_join_semi_anti_workspace(int64_t n_build, int64_t n_probe, int op);
+int pf_join_semi_anti(const int64_t* build_key, int64_t n_build, const int64_t* probe_key,
+                      int64_t n_probe, const int64_t* build_val, const int64_t* probe_val, int op,
+                      int anti, int64_t* out, int64_t* host_out, void* workspace,
+                      size_t workspace_bytes, void* stream);
+
+/*
+ * Sort/search pair expansion in two calls sharing one workspace:
+ * prepare scans len[0,m) and waits for the pair count (host_out[0]); run
+ * writes, for every probe row i and j < len[i], the pair
+ * (sorted_ids[start[i] + j], i) in probe-row order into cs / cr
+ * (host_out[0] rows each).
+ */
+size_t pf_join_expand_workspace(int64_t m);
+int pf_join_expand_prepare(const int64_t* len, int64_t m, int64_t* host_out, void* workspace,
+                           size_t workspace_bytes, void* stream);
+int pf_join_expand(const int64_t* sorted_ids, const int64_t* start, const int64_t* len, int64_t m,
+                   int64_t n_pairs, int64_t* cs, int64_t* cr, void* workspace,
+                   size_t workspace_bytes, void* stream);
+
+/* ---- dense slab group-by (DenseAggregationSlab) -------------------------- */
+#define PF_AGG_SUM 0
+#define PF_AGG_MAX 1
+#define PF_AGG_MIN 2
+#define PF_DT_I64 0
+#define PF_DT_F64 1
+#define PF_DT_I32 2
+/*
+ * Fold n rows into a direct-addressed slab over [key_min, key_min + capacity):
+ * occupied[key - key_min] = 1 and values[v][(key - key_min) * width[v] + e]
+ * op= src[v][row * width[v] + e].  keys are int64 (key_dtype PF_DT_I64) or
+ * int32 (PF_DT_I32); every key must lie in the range (rows outside it are
+ * counted into err_count, a device int64, and skipped).  Queued only.
+ */
+int pf_slab_add(const void* keys, int key_dtype, int64_t n, int64_t key_min, int64_t capacity,
+                uint8_t* occupied, int nvals, void* const* values, const void* const* srcs,
+                const int* dtypes, const int* ops, const int* widths, int64_t* err_count,
+                void* stream);
+/*
+ * The occupied slots, ascending: keys_out[j] = key_min + slot and
+ * vals_out[v][j] = values[v][slot] for the first host_out[0] rows (outputs
+ * sized for `capacity` rows).  Waits once.
+ */
+size_t pf_slab_finish_workspace(int64_t capacity);
+int pf_slab_finish(const uint8_t* occupied, int64_t key_min, int64_t capacity, int nvals,
+                   const void* const* values, const int* dtypes, const int* widths,
+                   int64_t* keys_out, void* const* vals_out, int64_t* host_out, void* workspace,
+                   size_t workspace_bytes, void* stream);
+
+/* ---- fused radix partition -> build/probe -> slab group-by --------------- */
+/*
+ * SELECT group, SUM(price * (scale - disc)), COUNT(*) FROM build JOIN probe
+ * ON build.key = probe.fk GROUP BY build.group, with a unique build key.
+ * Both sides are partitioned by the top log2(B) bits of mix64(key)
+ * (B a power of two in [1, 4096]), each partition's build rows go into an
+ * open-addressing table, and each matched probe row adds its value into a
+ * dense slab over [group_min, group_min + n_groups).  probe_disc may be NULL
+ * (the value is then price).  Sums are exact int64 (wrapping on overflow as
+ * int64 arithmetic does).  Outputs: sum_out / count_out [n_groups] (zero for
+ * groups no row reached; a group is present iff its count > 0) and, in
+ * stats_out (device int64[4]): matched probe rows, 0 (reserved), build rows
+ * whose group is out of range (their matches are not aggregated), and the
+ * number of build rows no table slot took (0 on success).  Waits once, for
+ * the bucket counts that plan the rounds; the rest stays queued.
+ */
+size_t pf_join_aggregate_workspace(int64_t n_build, int64_t n_probe, int B, int64_t n_groups);
+int pf_join_aggregate(const int64_t* build_key, const int32_t* build_group, int64_t n_build,
+                      const int64_t* probe_fk, const int64_t* probe_price,
+                      const int64_t* probe_disc, int64_t scale, int64_t n_probe, int B,
+                      int64_t group_min, int64_t n_groups, int64_t* sum_out, int64_t* count_out,
+                      int64_t* stats_out, void* workspace, size_t workspace_bytes, void* stream);
+/* The fan-out the autotuner seeds pf_join_aggregate with for these sizes. */
+int pf_join_aggregate_pick_b(int64_t n_build, int64_t n_probe);
+/*
+ * The groups a dense (sum, count) slab holds, ascending: keys_out[j] =
+ * group_min + g, sums_out[j] = sum[g], counts_out[j] = count[g] for every g
+ * with count[g] > 0; host_out[0] = their number (outputs sized n_groups).
+ * The finish of DenseAggregationSlab (operators/aggregation_slab.py:241-246)
+ * with COUNT as the occupancy.  Waits once.
+ */
+size_t pf_groups_finish_workspace(int64_t n_groups);
+int pf_groups_finish(const int64_t* sum, const int64_t* count, int64_t group_min,
+                     int64_t n_groups, int64_t* keys_out, int64_t* sums_out, int64_t* counts_out,
+                     int64_t* host_out, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- seeded synthetic inputs (identical to the CPU generator) ------------ */
+/* config ids: 0 = small (250K x 1M, 25 groups), 1 = scale (150M x 600M,
+ * 1.5M groups); `rows` and `lo` select rows [lo, lo + rows). */
+int pf_gen_build(int config, uint64_t seed, int64_t n_build, int64_t n_groups, int64_t lo,
+                 int64_t rows, int64_t* key, int32_t* group, void* stream);
+int pf_gen_probe(int config, uint64_t seed, int64_t n_build, int64_t lo, int64_t rows,
+                 int64_t* fk, int64_t* price, int64_t* disc, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PAGEFLOW_B200_H */

@@ -1,0 +1,230 @@
+"""ORACLE — test infrastructure only (tests/, __graft_entry__.smoke() and
+bench.py's CPU baseline import it; the product never does).
+
+A numpy front end over ``liboracle.so``, the plain-C restatement of
+PageFlow's semantics for the relational hot path (``oracle.c`` lists the
+reference lines each function follows).  Inputs and outputs are numpy arrays.
+Pinned by ``tests/golden`` (vectors produced by the reference's own Python
+code) in ``tests/test_oracle.py``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+
+_i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+_u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_c_i64 = ctypes.c_int64
+_lib = None
+
+
+def build() -> Path:
+    """Compiles liboracle.so when oracle.c or synth.h is newer."""
+    deps = [HERE / "oracle.c", HERE.parent / "pageflow_b200" / "csrc" / "synth.h"]
+    if not LIB.exists() or any(d.stat().st_mtime > LIB.stat().st_mtime for d in deps):
+        subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        L = ctypes.CDLL(str(LIB))
+        L.or_mix64.argtypes = [_i64p, _u64p, _c_i64]
+        L.or_bucket.argtypes = [_i64p, _c_i64, ctypes.c_int, _i32p]
+        L.or_partition_order.argtypes = [_i64p, _c_i64, ctypes.c_int, _i64p, _i64p]
+        L.or_partition_order.restype = ctypes.c_int
+        L.or_join_unique.argtypes = [_i64p, _i64p, _c_i64, _i64p, _i64p, _c_i64,
+                                     ctypes.c_int, _i64p, _i64p]
+        L.or_join_unique.restype = _c_i64
+        L.or_semi_anti.argtypes = [_i64p, ctypes.c_void_p, _c_i64, _i64p,
+                                   ctypes.c_void_p, _c_i64, ctypes.c_int,
+                                   ctypes.c_int, _i64p]
+        L.or_semi_anti.restype = _c_i64
+        L.or_join_aggregate.argtypes = [_i64p, _i32p, _c_i64, _i64p, _i64p,
+                                        ctypes.c_void_p, _c_i64, _c_i64, _c_i64,
+                                        _c_i64, ctypes.c_int, ctypes.c_int, _i64p,
+                                        _i64p, ctypes.POINTER(ctypes.c_uint64)]
+        L.or_join_aggregate.restype = _c_i64
+        L.or_gen_build.argtypes = [ctypes.c_uint64, _c_i64, _c_i64, _c_i64, _c_i64,
+                                   _i64p, _i32p]
+        L.or_gen_probe.argtypes = [ctypes.c_int, ctypes.c_uint64, _c_i64, _c_i64,
+                                   _c_i64, _i64p, _i64p, _i64p]
+        L.or_expected_groups.argtypes = [ctypes.c_int, ctypes.c_uint64, _c_i64,
+                                         _c_i64, _c_i64, _c_i64, _c_i64,
+                                         ctypes.c_int, _i64p, _i64p]
+        L.or_expected_groups.restype = _c_i64
+        _lib = L
+    return _lib
+
+
+def _a(x, dtype=np.int64):
+    return np.ascontiguousarray(x, dtype=dtype)
+
+
+def threads() -> int:
+    return max(1, len(os.sched_getaffinity(0)))
+
+
+# ---- hash and partition ----------------------------------------------------
+
+def mix64(keys) -> np.ndarray:
+    """Murmur3 fmix64 of int64 keys, as uint64."""
+    k = _a(keys)
+    out = np.empty(k.shape[0], np.uint64)
+    lib().or_mix64(k, out, k.shape[0])
+    return out
+
+
+def bucket(keys, B: int) -> np.ndarray:
+    """Each key's radix bucket among B: the top log2(B) bits of mix64."""
+    k = _a(keys)
+    out = np.empty(k.shape[0], np.int32)
+    lib().or_bucket(k, k.shape[0], B, out)
+    return out
+
+
+def rows_per_unit(row_bytes: int) -> int:
+    return 512 // int(np.gcd(int(row_bytes), 512))
+
+
+def partition(cols, key_pos: int, mask, goff: int, B: int):
+    """The reference test's partition: mask -> mix64 bucket -> stable sort
+    by bucket -> per-bucket split.  ``cols`` are raw (pre-mask) numpy
+    columns.  Returns (counts, outputs): one list of per-bucket arrays per
+    column, then the gidx's."""
+    n_pre = cols[key_pos].shape[0] if mask is None else mask.shape[0]
+    gidx = np.arange(goff, goff + n_pre, dtype=np.int64)
+    if mask is not None:
+        keep = np.asarray(mask).astype(bool)
+        cols = [c[keep] for c in cols]
+        gidx = gidx[keep]
+    key = _a(cols[key_pos])
+    counts = np.zeros(B, np.int64)
+    order = np.empty(key.shape[0], np.int64)
+    rc = lib().or_partition_order(key, key.shape[0], B, counts, order)
+    if rc:
+        raise ValueError(f"or_partition_order failed ({rc})")
+    bounds = np.cumsum(counts)[:-1]
+    outs = [np.split(c[order], bounds) for c in list(cols) + [gidx]]
+    return counts, outs
+
+
+def padded_layout(counts, row_b: int):
+    """Each bucket's first row and the total rows of the padded layout: a
+    non-empty bucket takes whole units of rows_per_unit(row_b) rows."""
+    unit = rows_per_unit(row_b)
+    starts, at = [], 0
+    for c in counts:
+        starts.append(at)
+        at += -(-int(c) // unit) * unit
+    return starts, at
+
+
+# ---- joins --------------------------------------------------------------------
+
+def join_unique(build_keys, probe_keys):
+    """(build rows, probe rows) of a unique-build inner join, probe order."""
+    nk = len(build_keys)
+    b0 = _a(build_keys[0])
+    b1 = _a(build_keys[1]) if nk == 2 else b0
+    p0 = _a(probe_keys[0])
+    p1 = _a(probe_keys[1]) if nk == 2 else p0
+    bi = np.empty(p0.shape[0], np.int64)
+    pi = np.empty(p0.shape[0], np.int64)
+    m = lib().or_join_unique(b0, b1, b0.shape[0], p0, p1, p0.shape[0], nk, bi, pi)
+    if m < 0:
+        raise MemoryError("or_join_unique")
+    return bi[:m], pi[:m]
+
+
+OPS = {None: 0, "<>": 1, "<": 2, "<=": 3, ">": 4, ">=": 5}
+
+
+def semi_anti(bk, pk, anti: bool, bv=None, pv=None, op=None):
+    """Probe rows, ascending, with (semi) or without (anti) a build row of
+    their key passing build.v OP probe.v."""
+    bk, pk = _a(bk), _a(pk)
+    bv_a = _a(bv) if bv is not None else None
+    pv_a = _a(pv) if pv is not None else None
+    out = np.empty(pk.shape[0], np.int64)
+    m = lib().or_semi_anti(
+        bk, bv_a.ctypes.data if bv_a is not None else None, bk.shape[0], pk,
+        pv_a.ctypes.data if pv_a is not None else None, pk.shape[0], OPS[op],
+        int(anti), out)
+    if m < 0:
+        raise MemoryError("or_semi_anti")
+    return out[:m]
+
+
+def expand(sorted_ids, start, length):
+    """The sort/search pairs: probe row i's run sorted_ids[start[i] :
+    start[i] + length[i]], in probe-row order."""
+    sorted_ids, start, length = _a(sorted_ids), _a(start), _a(length)
+    cr = np.repeat(np.arange(length.shape[0], dtype=np.int64), length)
+    first = np.repeat(start, length)
+    run0 = np.repeat(np.cumsum(length) - length, length)
+    within = np.arange(cr.shape[0], dtype=np.int64) - run0
+    return sorted_ids[first + within], cr
+
+
+def join_aggregate(bkey, bgrp, pfk, pprice, pdisc, scale: int, group_min: int,
+                   n_groups: int, B: int = 64, n_threads: int | None = None):
+    """Dense (sum, count) over [group_min, group_min + n_groups) of
+    SUM(price * (scale - disc)), COUNT(*) per build group of the
+    unique-build join; returns (sum, count, matched, max |sum|)."""
+    bkey, pfk, pprice = _a(bkey), _a(pfk), _a(pprice)
+    bgrp = _a(bgrp, np.int32)
+    pdisc_a = _a(pdisc) if pdisc is not None else None
+    s = np.empty(n_groups, np.int64)
+    c = np.empty(n_groups, np.int64)
+    mx = ctypes.c_uint64(0)
+    m = lib().or_join_aggregate(
+        bkey, bgrp, bkey.shape[0], pfk, pprice,
+        pdisc_a.ctypes.data if pdisc_a is not None else None, scale,
+        pfk.shape[0], group_min, n_groups, B, n_threads or threads(), s, c,
+        ctypes.byref(mx))
+    if m < 0:
+        raise MemoryError("or_join_aggregate")
+    return s, c, int(m), int(mx.value)
+
+
+# ---- workload generator ------------------------------------------------------
+
+def gen_build(seed: int, n_build: int, n_groups: int, lo: int = 0, rows=None):
+    rows = n_build - lo if rows is None else rows
+    key = np.empty(rows, np.int64)
+    grp = np.empty(rows, np.int32)
+    lib().or_gen_build(seed, n_build, n_groups, lo, rows, key, grp)
+    return key, grp
+
+
+def gen_probe(config: int, seed: int, n_build: int, lo: int, rows: int):
+    fk = np.empty(rows, np.int64)
+    price = np.empty(rows, np.int64)
+    disc = np.empty(rows, np.int64)
+    lib().or_gen_probe(config, seed, n_build, lo, rows, fk, price, disc)
+    return fk, price, disc
+
+
+def expected_groups(config: int, seed: int, n_build: int, n_groups: int,
+                    lo: int, rows: int, scale: int = 100, n_threads=None):
+    """Exact per-group (sum, count) of the workload's probe rows [lo, lo +
+    rows), from the generator alone; and the matched rows."""
+    s = np.empty(n_groups, np.int64)
+    c = np.empty(n_groups, np.int64)
+    m = lib().or_expected_groups(config, seed, n_build, n_groups, scale, lo,
+                                 rows, n_threads or threads(), s, c)
+    if m < 0:
+        raise MemoryError("or_expected_groups")
+    return s, c, int(m)

@@ -1,0 +1,426 @@
+/*
+ * ORACLE — test infrastructure only.  A plain-C restatement of PageFlow's
+ * CPU-visible semantics for the relational hot path, used by tests/ and by
+ * bench.py's CPU baseline as the checker and the reference arm; never by the
+ * product (pageflow_b200/), which runs on the GPU or fails.
+ *
+ * Pinned against golden vectors generated from the reference's own Python
+ * code (tests/golden/make_golden.py, run where the reference is importable):
+ * mix64 / bucket ids, the padded partition layout, the partition-count rule,
+ * the slab and sorted-run merge vectors, and the config-0 join + group-by
+ * result of the reference's KeyedAggregate.pass1 + reduce_tick_slice.
+ *
+ * Functions and the reference lines they follow:
+ *   or_mix64            operators/kernels/kernel_utils.cuh:18-22; tests/mix64.py:12-21
+ *   or_bucket           operators/aggregate.py:107-116; tests/mix64.py:30-36
+ *   or_partition_order  tests/operators/test_partition_sort.py:106-118 (mask ->
+ *                       mix64 bucket -> stable sort by bucket -> per-bucket split)
+ *   or_join_unique      operators/hashjoin.py:380-441 (_sort_search_pairs: per
+ *                       bucket sort of the build keys, searchsorted of each probe
+ *                       key; pairs in probe-row order) for a unique build tuple,
+ *                       operators/join_core.py:97-113
+ *   or_semi_anti        tests/operators/test_join_core.py:93-101 (a probe row is
+ *                       kept when some build row has its key and passes
+ *                       build.v OP probe.v; anti negates), ascending
+ *   or_join_aggregate   uvm/join.py:98-225 then uvm/aggregate.py:147-212: the
+ *                       inner join, then SUM / COUNT per group; SUM follows
+ *                       operators/operator_utils.py:389-398 (float64 bincount,
+ *                       rounded to int64), exact while every partial < 2^53,
+ *                       which the oracle checks and reports
+ *   or_expected_groups  the same join + group-by computed from the generator
+ *                       alone (the inverse of the build-key permutation gives
+ *                       each FK's build row), for full-size checks
+ *   or_gen_build/probe  the CPU twin of the CUDA generator (synth.h)
+ */
+#define _GNU_SOURCE
+#include <pthread.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "../pageflow_b200/csrc/synth.h"
+
+/* ---- mix64 and buckets ---------------------------------------------------- */
+
+static inline uint64_t mix64(uint64_t k) {
+  k ^= k >> 33;
+  k *= 0xff51afd7ed558ccdULL;
+  k ^= k >> 33;
+  k *= 0xc4ceb9fe1a85ec53ULL;
+  k ^= k >> 33;
+  return k;
+}
+
+static inline int log2i(int64_t b) {
+  int l = 0;
+  while ((1LL << l) < b) ++l;
+  return l;
+}
+
+static inline int bucket(int64_t key, int logb) {
+  return logb ? (int)(mix64((uint64_t)key) >> (64 - logb)) : 0;
+}
+
+void or_mix64(const int64_t* in, uint64_t* out, int64_t n) {
+  for (int64_t i = 0; i < n; ++i) out[i] = mix64((uint64_t)in[i]);
+}
+
+void or_bucket(const int64_t* keys, int64_t n, int B, int32_t* out) {
+  const int lb = log2i(B);
+  for (int64_t i = 0; i < n; ++i) out[i] = bucket(keys[i], lb);
+}
+
+/* Stable partition of n keys into B buckets: counts[B] and order[n], the rows
+ * sorted by bucket, source order kept inside a bucket (a counting sort, which
+ * is the stable sort of the reference test). */
+int or_partition_order(const int64_t* keys, int64_t n, int B, int64_t* counts, int64_t* order) {
+  if (B < 1 || (B & (B - 1))) return -1;
+  const int lb = log2i(B);
+  int32_t* bk = (int32_t*)malloc(sizeof(int32_t) * (n > 0 ? n : 1));
+  int64_t* at = (int64_t*)calloc((size_t)B, sizeof(int64_t));
+  if (!bk || !at) {
+    free(bk);
+    free(at);
+    return -2;
+  }
+  memset(counts, 0, sizeof(int64_t) * B);
+  for (int64_t i = 0; i < n; ++i) {
+    bk[i] = bucket(keys[i], lb);
+    counts[bk[i]]++;
+  }
+  int64_t s = 0;
+  for (int b = 0; b < B; ++b) {
+    at[b] = s;
+    s += counts[b];
+  }
+  for (int64_t i = 0; i < n; ++i) order[at[bk[i]]++] = i;
+  free(bk);
+  free(at);
+  return 0;
+}
+
+/* ---- sort helpers --------------------------------------------------------- */
+
+typedef struct {
+  int64_t k0, k1, v;
+  int64_t row;
+} rec_t;
+
+static int cmp_rec(const void* a, const void* b) {
+  const rec_t* x = (const rec_t*)a;
+  const rec_t* y = (const rec_t*)b;
+  if (x->k0 != y->k0) return x->k0 < y->k0 ? -1 : 1;
+  if (x->k1 != y->k1) return x->k1 < y->k1 ? -1 : 1;
+  if (x->row != y->row) return x->row < y->row ? -1 : 1;
+  return 0;
+}
+
+/* First index in r[0,n) whose (k0,k1) >= (a,b). */
+static int64_t lower(const rec_t* r, int64_t n, int64_t a, int64_t b) {
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (r[mid].k0 < a || (r[mid].k0 == a && r[mid].k1 < b)) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+/* ---- unique-build inner join --------------------------------------------- */
+
+/* (build_idx, probe_idx) of every probe row whose tuple is in the build, in
+ * probe-row order; returns their number (or < 0 on allocation failure).  A
+ * probe row takes the first build row (in build order) with its tuple. */
+int64_t or_join_unique(const int64_t* b0, const int64_t* b1, int64_t nb, const int64_t* p0,
+                       const int64_t* p1, int64_t np, int nkeys, int64_t* build_idx,
+                       int64_t* probe_idx) {
+  rec_t* r = (rec_t*)malloc(sizeof(rec_t) * (nb > 0 ? nb : 1));
+  if (!r) return -1;
+  for (int64_t i = 0; i < nb; ++i) {
+    r[i].k0 = b0[i];
+    r[i].k1 = nkeys == 2 ? b1[i] : 0;
+    r[i].v = 0;
+    r[i].row = i;
+  }
+  qsort(r, (size_t)nb, sizeof(rec_t), cmp_rec);
+  int64_t m = 0;
+  for (int64_t i = 0; i < np; ++i) {
+    const int64_t a = p0[i], b = nkeys == 2 ? p1[i] : 0;
+    const int64_t j = lower(r, nb, a, b);
+    if (j < nb && r[j].k0 == a && r[j].k1 == b) {
+      build_idx[m] = r[j].row;
+      probe_idx[m] = i;
+      ++m;
+    }
+  }
+  free(r);
+  return m;
+}
+
+/* ---- semi / anti ----------------------------------------------------------- */
+
+/* op: 0 none, 1 <>, 2 <, 3 <=, 4 >, 5 >= (build.v OP probe.v). */
+int64_t or_semi_anti(const int64_t* bk, const int64_t* bv, int64_t nb, const int64_t* pk,
+                     const int64_t* pv, int64_t np, int op, int anti, int64_t* out) {
+  rec_t* r = (rec_t*)malloc(sizeof(rec_t) * (nb > 0 ? nb : 1));
+  if (!r) return -1;
+  for (int64_t i = 0; i < nb; ++i) {
+    r[i].k0 = bk[i];
+    r[i].k1 = 0;
+    r[i].v = bv ? bv[i] : 0;
+    r[i].row = i;
+  }
+  qsort(r, (size_t)nb, sizeof(rec_t), cmp_rec);
+  int64_t m = 0;
+  for (int64_t i = 0; i < np; ++i) {
+    int64_t j = lower(r, nb, pk[i], 0);
+    int hit = 0;
+    for (; j < nb && r[j].k0 == pk[i] && !hit; ++j) {
+      if (op == 0) {
+        hit = 1;
+      } else {
+        const int64_t a = r[j].v, b = pv[i];
+        switch (op) {
+          case 1: hit = a != b; break;
+          case 2: hit = a < b; break;
+          case 3: hit = a <= b; break;
+          case 4: hit = a > b; break;
+          default: hit = a >= b; break;
+        }
+      }
+    }
+    if (hit != (anti != 0)) out[m++] = i;
+  }
+  free(r);
+  return m;
+}
+
+/* ---- join + group-by ---------------------------------------------------------- */
+
+typedef struct {
+  const int64_t *bkey, *pfk, *pprice, *pdisc;
+  const int32_t* bgrp;
+  int64_t scale, gmin, ngroups;
+  const int64_t *bstart, *pstart; /* per bucket row ranges of the partitioned sides */
+  const int64_t *border, *porder;
+  int B, b0, b1;                  /* this worker's buckets */
+  int64_t* sum;                   /* private [ngroups] */
+  int64_t* count;                 /* private [ngroups] */
+  int64_t matched;
+  int rc;
+} jw_t;
+
+static void* join_worker(void* arg) {
+  jw_t* w = (jw_t*)arg;
+  int64_t cap = 0;
+  rec_t* r = NULL;
+  for (int b = w->b0; b < w->b1; ++b) {
+    const int64_t n = w->bstart[b + 1] - w->bstart[b];
+    if (n > cap) {
+      free(r);
+      cap = n;
+      r = (rec_t*)malloc(sizeof(rec_t) * (size_t)cap);
+      if (!r) {
+        w->rc = -1;
+        return NULL;
+      }
+    }
+    for (int64_t j = 0; j < n; ++j) {
+      const int64_t row = w->border[w->bstart[b] + j];
+      r[j].k0 = w->bkey[row];
+      r[j].k1 = 0;
+      r[j].v = w->bgrp[row];
+      r[j].row = row;
+    }
+    qsort(r, (size_t)n, sizeof(rec_t), cmp_rec);
+    for (int64_t q = w->pstart[b]; q < w->pstart[b + 1]; ++q) {
+      const int64_t row = w->porder[q];
+      const int64_t k = w->pfk[row];
+      const int64_t j = lower(r, n, k, 0);
+      if (j < n && r[j].k0 == k) {
+        const int64_t g = r[j].v - w->gmin;
+        w->matched++;
+        if (g < 0 || g >= w->ngroups) continue;
+        const int64_t v = w->pdisc ? (int64_t)((uint64_t)w->pprice[row] *
+                                               (uint64_t)(w->scale - w->pdisc[row]))
+                                   : w->pprice[row];
+        w->sum[g] = (int64_t)((uint64_t)w->sum[g] + (uint64_t)v);
+        w->count[g]++;
+      }
+    }
+  }
+  free(r);
+  return NULL;
+}
+
+/* SELECT group, SUM(price * (scale - disc)), COUNT(*) over the unique-build
+ * join, into dense sum / count arrays over [gmin, gmin + ngroups).  Both sides
+ * are partitioned into B buckets by mix64 (the reference's layout), buckets
+ * are joined by sort + binary search on `threads` threads.  Returns the
+ * matched probe rows; *max_abs gets the largest |group sum| (the reference's
+ * float64 SUM is exact below 2^53).  < 0 on failure. */
+int64_t or_join_aggregate(const int64_t* bkey, const int32_t* bgrp, int64_t nb,
+                          const int64_t* pfk, const int64_t* pprice, const int64_t* pdisc,
+                          int64_t scale, int64_t np, int64_t gmin, int64_t ngroups, int B,
+                          int threads, int64_t* sum, int64_t* count, uint64_t* max_abs) {
+  if (threads < 1) threads = 1;
+  if (B < 1) B = 1;
+  int64_t* bc = (int64_t*)malloc(sizeof(int64_t) * B);
+  int64_t* pc = (int64_t*)malloc(sizeof(int64_t) * B);
+  int64_t* bs = (int64_t*)malloc(sizeof(int64_t) * (B + 1));
+  int64_t* ps = (int64_t*)malloc(sizeof(int64_t) * (B + 1));
+  int64_t* bo = (int64_t*)malloc(sizeof(int64_t) * (nb > 0 ? nb : 1));
+  int64_t* po = (int64_t*)malloc(sizeof(int64_t) * (np > 0 ? np : 1));
+  jw_t* ws = (jw_t*)calloc((size_t)threads, sizeof(jw_t));
+  pthread_t* th = (pthread_t*)calloc((size_t)threads, sizeof(pthread_t));
+  int64_t result = -1;
+  if (!bc || !pc || !bs || !ps || !bo || !po || !ws || !th) goto done;
+  if (or_partition_order(bkey, nb, B, bc, bo) || or_partition_order(pfk, np, B, pc, po)) goto done;
+  bs[0] = ps[0] = 0;
+  for (int b = 0; b < B; ++b) {
+    bs[b + 1] = bs[b] + bc[b];
+    ps[b + 1] = ps[b] + pc[b];
+  }
+  for (int t = 0; t < threads; ++t) {
+    jw_t* w = &ws[t];
+    w->bkey = bkey;
+    w->bgrp = bgrp;
+    w->pfk = pfk;
+    w->pprice = pprice;
+    w->pdisc = pdisc;
+    w->scale = scale;
+    w->gmin = gmin;
+    w->ngroups = ngroups;
+    w->bstart = bs;
+    w->pstart = ps;
+    w->border = bo;
+    w->porder = po;
+    w->B = B;
+    w->b0 = (int)((int64_t)B * t / threads);
+    w->b1 = (int)((int64_t)B * (t + 1) / threads);
+    w->sum = (int64_t*)calloc((size_t)ngroups, sizeof(int64_t));
+    w->count = (int64_t*)calloc((size_t)ngroups, sizeof(int64_t));
+    if (!w->sum || !w->count) goto done;
+  }
+  for (int t = 0; t < threads; ++t) pthread_create(&th[t], NULL, join_worker, &ws[t]);
+  for (int t = 0; t < threads; ++t) pthread_join(th[t], NULL);
+  memset(sum, 0, sizeof(int64_t) * ngroups);
+  memset(count, 0, sizeof(int64_t) * ngroups);
+  int64_t matched = 0;
+  for (int t = 0; t < threads; ++t) {
+    if (ws[t].rc) goto done;
+    matched += ws[t].matched;
+    for (int64_t g = 0; g < ngroups; ++g) {
+      sum[g] = (int64_t)((uint64_t)sum[g] + (uint64_t)ws[t].sum[g]);
+      count[g] += ws[t].count[g];
+    }
+  }
+  uint64_t mx = 0;
+  for (int64_t g = 0; g < ngroups; ++g) {
+    const uint64_t a = sum[g] < 0 ? (uint64_t)(-(sum[g] + 1)) + 1 : (uint64_t)sum[g];
+    if (a > mx) mx = a;
+  }
+  if (max_abs) *max_abs = mx;
+  result = matched;
+done:
+  if (ws)
+    for (int t = 0; t < threads; ++t) {
+      free(ws[t].sum);
+      free(ws[t].count);
+    }
+  free(bc);
+  free(pc);
+  free(bs);
+  free(ps);
+  free(bo);
+  free(po);
+  free(ws);
+  free(th);
+  return result;
+}
+
+/* ---- generator --------------------------------------------------------------- */
+
+void or_gen_build(uint64_t seed, int64_t n_build, int64_t n_groups, int64_t lo, int64_t rows,
+                  int64_t* key, int32_t* group) {
+  const pf_perm_t perm = pf_perm_make(seed, (uint64_t)n_build);
+  for (int64_t i = 0; i < rows; ++i)
+    pf_gen_build_row(seed, (uint64_t)n_build, (uint64_t)n_groups, &perm, (uint64_t)(lo + i),
+                     &key[i], &group[i]);
+}
+
+void or_gen_probe(int config, uint64_t seed, int64_t n_build, int64_t lo, int64_t rows,
+                  int64_t* fk, int64_t* price, int64_t* disc) {
+  const int miss = pf_cfg_miss_per_10(config);
+  for (int64_t i = 0; i < rows; ++i)
+    pf_gen_probe_row(seed, (uint64_t)n_build, miss, (uint64_t)(lo + i), &fk[i], &price[i],
+                     &disc[i]);
+}
+
+typedef struct {
+  int config;
+  uint64_t seed;
+  int64_t n_build, n_groups, lo, hi;
+  int64_t scale;
+  const pf_perm_t* perm;
+  int64_t *sum, *count, matched;
+} ew_t;
+
+static void* expect_worker(void* arg) {
+  ew_t* w = (ew_t*)arg;
+  const int miss = pf_cfg_miss_per_10(w->config);
+  for (int64_t r = w->lo; r < w->hi; ++r) {
+    int64_t fk, price, disc;
+    pf_gen_probe_row(w->seed, (uint64_t)w->n_build, miss, (uint64_t)r, &fk, &price, &disc);
+    if (fk < 1 || fk > w->n_build) continue;
+    const uint64_t brow = pf_perm_inv(w->perm, (uint64_t)(fk - 1));
+    const int64_t g = (int64_t)pf_range(pf_u(w->seed, 1, brow), (uint64_t)w->n_groups);
+    w->sum[g] = (int64_t)((uint64_t)w->sum[g] + (uint64_t)price * (uint64_t)(w->scale - disc));
+    w->count[g]++;
+    w->matched++;
+  }
+  return NULL;
+}
+
+/* The workload's exact per-group SUM(price * (scale - disc)) and COUNT over
+ * probe rows [lo, lo + rows), from the generator: FK f matches build row
+ * perm^-1(f - 1), whose group the generator gives.  Returns matched rows. */
+int64_t or_expected_groups(int config, uint64_t seed, int64_t n_build, int64_t n_groups,
+                           int64_t scale, int64_t lo, int64_t rows, int threads, int64_t* sum,
+                           int64_t* count) {
+  if (threads < 1) threads = 1;
+  const pf_perm_t perm = pf_perm_make(seed, (uint64_t)n_build);
+  ew_t* ws = (ew_t*)calloc((size_t)threads, sizeof(ew_t));
+  pthread_t* th = (pthread_t*)calloc((size_t)threads, sizeof(pthread_t));
+  if (!ws || !th) return -1;
+  for (int t = 0; t < threads; ++t) {
+    ws[t].config = config;
+    ws[t].seed = seed;
+    ws[t].n_build = n_build;
+    ws[t].n_groups = n_groups;
+    ws[t].scale = scale;
+    ws[t].perm = &perm;
+    ws[t].lo = lo + rows * t / threads;
+    ws[t].hi = lo + rows * (t + 1) / threads;
+    ws[t].sum = (int64_t*)calloc((size_t)n_groups, sizeof(int64_t));
+    ws[t].count = (int64_t*)calloc((size_t)n_groups, sizeof(int64_t));
+    if (!ws[t].sum || !ws[t].count) return -1;
+  }
+  for (int t = 0; t < threads; ++t) pthread_create(&th[t], NULL, expect_worker, &ws[t]);
+  for (int t = 0; t < threads; ++t) pthread_join(th[t], NULL);
+  memset(sum, 0, sizeof(int64_t) * n_groups);
+  memset(count, 0, sizeof(int64_t) * n_groups);
+  int64_t matched = 0;
+  for (int t = 0; t < threads; ++t) {
+    for (int64_t g = 0; g < n_groups; ++g) {
+      sum[g] = (int64_t)((uint64_t)sum[g] + (uint64_t)ws[t].sum[g]);
+      count[g] += ws[t].count[g];
+    }
+    matched += ws[t].matched;
+    free(ws[t].sum);
+    free(ws[t].count);
+  }
+  free(ws);
+  free(th);
+  return matched;
+}

@@ -1,0 +1,754 @@
+// The fused join -> group-by of one unique-build FK join, sm_100a:
+//
+//   SELECT b.group, SUM(p.price * (scale - p.disc)), COUNT(*)
+//   FROM build b JOIN probe p ON b.key = p.fk GROUP BY b.group
+//
+// It replaces the reference's composition of partition_sort per morsel ->
+// join_unique_hash per bucket pair -> index_select -> KeyedAggregate.pass1 ->
+// reduce_tick_slice (uvm/join.py:98-225, uvm/aggregate.py:147-212), whose
+// every step is an HBM round trip, with four passes:
+//
+//   1. k_fhist      per-chunk bucket histograms of both sides' keys
+//   2. k_fscan      per bucket, each chunk's offset (then the bucket starts)
+//   3. k_fscatter   radix scatter of both sides into bucket order; the probe
+//                   side carries (fk, value) with value = price * (scale -
+//                   disc) computed on the way, so the price and discount
+//                   columns are read once and never written
+//   4. per round    k_fbuild: the round's build rows into an open-addressing
+//                   table in L2 (16-byte slots {key, group | round tag});
+//                   k_fprobe: each probe row of the round's partitions looks
+//                   its key up and adds its value and 1 into the dense group
+//                   slab (sum, count) with fire-and-forget atomics
+//
+// A row's bucket is the top log2(B) bits of mix64(key), as in the reference's
+// partition kernel.  A round is a run of whole partitions whose build rows fit
+// the table budget (each partition owns a region of twice its build rows,
+// load <= 0.5), or one slice of a partition too large for it (its probe rows
+// then meet every slice; a unique build key lives in exactly one).  Slots carry
+// the round's tag, so the table is cleared once per call, not per round.
+// The bucket counts come to the host once, to plan the rounds.
+#include <algorithm>
+#include <vector>
+
+#include "scan.cuh"
+
+namespace pf {
+namespace {
+
+constexpr int FT = 512;            // threads of the histogram and scatter
+constexpr int FITEMS = 8;
+constexpr int FSUB = FT * FITEMS;  // rows of a scatter sub-tile
+constexpr int FB_MAX = 4096;       // fan-out limit
+constexpr int PT2 = 256;           // threads of build / probe
+constexpr int PITEMS2 = 4;         // rows a probe thread keeps in flight
+constexpr long long ROUND_ROWS_DEFAULT = 1536 * 1024;  // build rows a round's table holds
+
+struct Slot {
+  unsigned long long key;
+  unsigned long long tagged;  // (tag << 32) | group offset
+};
+
+__device__ __forceinline__ Slot load_slot(const Slot* p) {
+  const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(p);
+  return Slot{v.x, v.y};
+}
+
+// ---- 1. histograms ------------------------------------------------------------
+
+__global__ void __launch_bounds__(FT) k_fhist(const long long* __restrict__ key, long long n,
+                                              long long chunk, int logB, int B,
+                                              int* __restrict__ hist) {
+  extern __shared__ int h[];
+  for (int b = threadIdx.x; b < B; b += FT) h[b] = 0;
+  __syncthreads();
+  const long long lo = (long long)blockIdx.x * chunk;
+  const long long hi = min(n, lo + chunk);
+  for (long long i = lo + threadIdx.x; i < hi; i += FT) {
+    const int b = bucket_of_hash(mix64((uint64_t)key[i]), logB);
+    atomicAdd(&h[b], 1);
+  }
+  __syncthreads();
+  int* row = hist + (long long)blockIdx.x * B;
+  for (int b = threadIdx.x; b < B; b += FT) row[b] = h[b];
+}
+
+// ---- 2. per-bucket chunk offsets ------------------------------------------------
+
+// Block g owns buckets [32g, 32g + 32); warp j scans chunks [j*per, ...).
+// hist becomes each chunk's offset inside its bucket; counts[b] the bucket's
+// rows.
+__global__ void __launch_bounds__(FT) k_fscan(int* __restrict__ hist, int nchunks, int B,
+                                              long long* __restrict__ counts) {
+  constexpr int W = FT / 32;
+  __shared__ long long part[W][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int b = blockIdx.x * 32 + lane;
+  const bool live = b < B;
+  const int per = (nchunks + W - 1) / W;
+  const int c0 = w * per, c1 = min(nchunks, c0 + per);
+  long long s = 0;
+  if (live)
+    for (int c = c0; c < c1; ++c) s += hist[(long long)c * B + b];
+  part[w][lane] = s;
+  __syncthreads();
+  if (w == 0) {
+    long long run = 0;
+    for (int j = 0; j < W; ++j) {
+      const long long t = part[j][lane];
+      part[j][lane] = run;
+      run += t;
+    }
+    if (live) counts[b] = run;
+  }
+  __syncthreads();
+  if (live) {
+    long long run = part[w][lane];
+    for (int c = c0; c < c1; ++c) {
+      const long long i = (long long)c * B + b;
+      const int t = hist[i];
+      hist[i] = (int)run;
+      run += t;
+    }
+  }
+}
+
+// ---- 3. the scatter ---------------------------------------------------------------
+
+// VAL: the carried value's type (int for the build side's group, long long for
+// the probe side's computed value).
+template <bool PROBE>
+__global__ void __launch_bounds__(FT) k_fscatter(const long long* __restrict__ key,
+                                                 const void* __restrict__ v0,
+                                                 const long long* __restrict__ v1,
+                                                 long long scale, long long n, long long chunk,
+                                                 int logB, int B, const int* __restrict__ hist,
+                                                 const long long* __restrict__ start,
+                                                 long long* __restrict__ okey,
+                                                 void* __restrict__ oval) {
+  using V = typename std::conditional<PROBE, long long, int>::type;
+  extern __shared__ __align__(16) unsigned char smem[];
+  long long* base = reinterpret_cast<long long*>(smem);           // [B]
+  int* cnt = reinterpret_cast<int*>(base + B);                     // [B]
+  int* tstart = cnt + B;                                           // [B]
+  int* wsum = tstart + B;                                          // [32]
+  unsigned long long* skey = reinterpret_cast<unsigned long long*>(
+      smem + ((size_t)B * 16 + 32 * 4 + 15) / 16 * 16);            // [FSUB]
+  V* sval = reinterpret_cast<V*>(skey + FSUB);                     // [FSUB]
+  unsigned short* sbk = reinterpret_cast<unsigned short*>(sval + FSUB);  // [FSUB]
+
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int* hrow = hist + (long long)blockIdx.x * B;
+  for (int b = tid; b < B; b += FT) base[b] = start[b] + hrow[b];
+  const long long lo = (long long)blockIdx.x * chunk;
+  const long long hi = min(n, lo + chunk);
+  const V* in0 = reinterpret_cast<const V*>(v0);
+  V* out0 = reinterpret_cast<V*>(oval);
+
+  for (long long sb = lo; sb < hi; sb += FSUB) {
+    for (int b = tid; b < B; b += FT) cnt[b] = 0;
+    __syncthreads();
+    long long kv[FITEMS];
+    V vv[FITEMS];
+    int bk[FITEMS], rk[FITEMS];
+#pragma unroll
+    for (int k = 0; k < FITEMS; ++k) {
+      const long long i = sb + k * FT + tid;
+      bk[k] = -1;
+      if (i < hi) {
+        kv[k] = key[i];
+        if (PROBE) {
+          const long long price = reinterpret_cast<const long long*>(v0)[i];
+          vv[k] = (V)(v1 ? (long long)((unsigned long long)price *
+                                       (unsigned long long)(scale - v1[i]))
+                         : price);
+        } else {
+          vv[k] = in0[i];
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < FITEMS; ++k) {
+      const long long i = sb + k * FT + tid;
+      if (i < hi) {
+        bk[k] = bucket_of_hash(mix64((uint64_t)kv[k]), logB);
+        rk[k] = atomicAdd(&cnt[bk[k]], 1);
+      }
+    }
+    __syncthreads();
+    // exclusive scan of cnt into tstart (each thread a run of buckets)
+    {
+      const int per = (B + FT - 1) / FT;
+      const int b0 = tid * per;
+      int s = 0;
+      for (int q = 0; q < per; ++q)
+        if (b0 + q < B) s += cnt[b0 + q];
+      int incl = s;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += y;
+      }
+      if (lane == 31) wsum[w] = incl;
+      __syncthreads();
+      int pre = 0;
+      for (int q = 0; q < FT / 32; ++q) pre += q < w ? wsum[q] : 0;
+      int ex = pre + incl - s;
+      for (int q = 0; q < per; ++q) {
+        if (b0 + q < B) {
+          tstart[b0 + q] = ex;
+          ex += cnt[b0 + q];
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < FITEMS; ++k) {
+      if (bk[k] >= 0) {
+        const int s = tstart[bk[k]] + rk[k];
+        skey[s] = (unsigned long long)kv[k];
+        sval[s] = vv[k];
+        sbk[s] = (unsigned short)bk[k];
+      }
+    }
+    __syncthreads();
+    const int nsub = (int)min((long long)FSUB, hi - sb);
+    for (int s = tid; s < nsub; s += FT) {
+      const int b = sbk[s];
+      const long long pos = base[b] + (s - tstart[b]);
+      okey[pos] = (long long)skey[s];
+      out0[pos] = sval[s];
+    }
+    __syncthreads();
+    for (int b = tid; b < B; b += FT) base[b] += cnt[b];
+    __syncthreads();
+  }
+}
+
+size_t fscatter_smem(int B, bool probe) {
+  size_t s = ((size_t)B * 16 + 32 * 4 + 15) / 16 * 16;
+  s += (size_t)FSUB * 8;                // skey
+  s += (size_t)FSUB * (probe ? 8 : 4);  // sval
+  s += (size_t)FSUB * 2;                // sbk
+  return s;
+}
+
+// ---- 4. rounds: build and probe ----------------------------------------------------
+
+struct RoundArgs {
+  const long long* bkey;  // partitioned build keys
+  const int* bgrp;        // partitioned build groups
+  long long b_lo, b_hi;   // the round's build rows
+  const long long* pfk;   // partitioned probe keys
+  const long long* pval;  // partitioned probe values
+  long long p_lo, p_hi;   // the round's probe rows
+  Slot* table;
+  const long long* reg_off;  // [B] slot offset of each partition's region
+  const long long* reg_cap;  // [B] slots of each partition's region
+  long long slice_cap;       // > 0: a slice round, one region of this size at 0
+  unsigned tag;
+  int logB;
+  long long group_min, n_groups;
+  unsigned long long* sum;
+  unsigned long long* count;
+  unsigned long long* stats;  // [0] matched, [1] reserved, [2] build rows out of group range, [3] overflow
+};
+
+__device__ __forceinline__ void region_of(const RoundArgs& a, uint64_t h, long long* off,
+                                          long long* cap) {
+  if (a.slice_cap > 0) {
+    *off = 0;
+    *cap = a.slice_cap;
+  } else {
+    const int b = bucket_of_hash(h, a.logB);
+    *off = a.reg_off[b];
+    *cap = a.reg_cap[b];
+  }
+}
+
+// The first slot of hash h inside a region of `cap` slots: multiply-shift of
+// the 32 bits right below the bucket bits.
+__device__ __forceinline__ long long first_slot(uint64_t h, int logB, long long cap) {
+  const uint32_t x = (uint32_t)((h << logB) >> 32);
+  return (long long)(((unsigned long long)x * (unsigned long long)cap) >> 32);
+}
+
+__global__ void __launch_bounds__(PT2) k_fbuild(RoundArgs a) {
+  unsigned long long bad_group = 0, overflow = 0;
+  for (long long i = a.b_lo + (long long)blockIdx.x * PT2 + threadIdx.x; i < a.b_hi;
+       i += (long long)gridDim.x * PT2) {
+    const long long k = a.bkey[i];
+    const long long g = (long long)a.bgrp[i] - a.group_min;
+    uint32_t goff = 0xffffffffu;
+    if (g >= 0 && g < a.n_groups) goff = (uint32_t)g;
+    else ++bad_group;
+    const uint64_t h = mix64((uint64_t)k);
+    long long off, cap;
+    region_of(a, h, &off, &cap);
+    long long s = first_slot(h, a.logB, cap);
+    const unsigned long long mine = ((unsigned long long)a.tag << 32) | goff;
+    bool done = false;
+    for (long long probes = 0; probes < cap; ++probes) {
+      Slot* sl = a.table + off + s;
+      unsigned long long cur = sl->tagged;
+      if ((uint32_t)(cur >> 32) != a.tag) {
+        if (atomicCAS(&sl->tagged, cur, mine) == cur) {
+          sl->key = (unsigned long long)k;
+          done = true;
+          break;
+        }
+      }
+      if (++s == cap) s = 0;
+    }
+    overflow += !done;
+  }
+  if (bad_group) atomicAdd(&a.stats[2], bad_group);
+  if (overflow) atomicAdd(&a.stats[3], overflow);
+}
+
+__global__ void __launch_bounds__(PT2) k_fprobe(RoundArgs a) {
+  unsigned long long matched = 0;
+  const long long stride = (long long)gridDim.x * PT2 * PITEMS2;
+  for (long long i0 = a.p_lo + ((long long)blockIdx.x * PT2 * PITEMS2) + threadIdx.x;
+       i0 < a.p_hi; i0 += stride) {
+    long long key[PITEMS2], val[PITEMS2], off[PITEMS2], cap[PITEMS2], s[PITEMS2];
+    Slot sl[PITEMS2];
+#pragma unroll
+    for (int k = 0; k < PITEMS2; ++k) {
+      const long long i = i0 + (long long)k * PT2;
+      cap[k] = 0;
+      if (i < a.p_hi) {
+        key[k] = a.pfk[i];
+        val[k] = a.pval[i];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < PITEMS2; ++k) {
+      const long long i = i0 + (long long)k * PT2;
+      if (i < a.p_hi) {
+        const uint64_t h = mix64((uint64_t)key[k]);
+        region_of(a, h, &off[k], &cap[k]);
+        if (cap[k] > 0) {
+          s[k] = first_slot(h, a.logB, cap[k]);
+          sl[k] = load_slot(a.table + off[k] + s[k]);
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < PITEMS2; ++k) {
+      if (cap[k] <= 0) continue;
+      long long probes = 0;
+      while (true) {
+        if ((uint32_t)(sl[k].tagged >> 32) != a.tag) break;  // a free slot: no match
+        if (sl[k].key == (unsigned long long)key[k]) {
+          const uint32_t g = (uint32_t)sl[k].tagged;
+          if (g != 0xffffffffu) {
+            atomicAdd(&a.sum[g], (unsigned long long)val[k]);
+            atomicAdd(&a.count[g], 1ULL);
+          }
+          ++matched;
+          break;
+        }
+        if (++probes >= cap[k]) break;
+        if (++s[k] == cap[k]) s[k] = 0;
+        sl[k] = load_slot(a.table + off[k] + s[k]);
+      }
+    }
+  }
+  for (int o = 16; o; o >>= 1) matched += __shfl_xor_sync(FULL, matched, o);
+  if ((threadIdx.x & 31) == 0 && matched) atomicAdd(&a.stats[0], matched);
+}
+
+// The regions of the rounds, from the build counts: the same greedy packing
+// as the host's plan (one thread; B <= 4096).  A partition over the budget
+// gets no region here (its slice rounds pass their own).
+__global__ void k_plan(const long long* __restrict__ cnt, int B, long long cap_rows,
+                       long long* __restrict__ reg) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  long long rows = 0;
+  for (int p = 0; p < B; ++p) {
+    const long long n = cnt[p];
+    if (n > cap_rows) {
+      reg[p] = 0;
+      reg[B + p] = 0;
+      rows = 0;
+      continue;
+    }
+    if (rows + n > cap_rows) rows = 0;
+    reg[p] = 2 * rows;
+    reg[B + p] = 2 * n;
+    rows += n;
+  }
+}
+
+// ---- finish: the groups present, ascending ------------------------------------------
+
+__global__ void __launch_bounds__(CT) k_gcount(const long long* __restrict__ count, long long n,
+                                               long long* __restrict__ bcnt) {
+  const long long base = (long long)blockIdx.x * CB;
+  int c = 0;
+  for (int k = 0; k < CITEMS; ++k) {
+    const long long i = base + k * CT + threadIdx.x;
+    if (i < n) c += count[i] > 0;
+  }
+  __shared__ int red[CT / 32];
+  for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(FULL, c, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int q = 0; q < CT / 32; ++q) t += red[q];
+    bcnt[blockIdx.x] = t;
+  }
+}
+
+__global__ void __launch_bounds__(CT) k_gemit(const long long* __restrict__ sum,
+                                              const long long* __restrict__ count, long long n,
+                                              long long group_min,
+                                              const long long* __restrict__ boff,
+                                              long long* __restrict__ keys,
+                                              long long* __restrict__ sums,
+                                              long long* __restrict__ counts) {
+  __shared__ int wsum[CT / 32];
+  const long long base = (long long)blockIdx.x * CB + (long long)threadIdx.x * CITEMS;
+  bool kp[CITEMS];
+  int rank[CITEMS];
+#pragma unroll
+  for (int k = 0; k < CITEMS; ++k) kp[k] = base + k < n && count[base + k] > 0;
+  block_ranks(kp, rank, wsum);
+  const long long o = boff[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < CITEMS; ++k) {
+    if (kp[k]) {
+      const long long j = o + rank[k];
+      keys[j] = group_min + base + k;
+      sums[j] = sum[base + k];
+      counts[j] = count[base + k];
+    }
+  }
+}
+
+// ---- host ------------------------------------------------------------------------------
+
+long long round_rows() {
+  static long long v = [] {
+    const char* e = getenv("PF_ROUND_ROWS");
+    long long x = e ? atoll(e) : 0;
+    return x > 0 ? x : ROUND_ROWS_DEFAULT;
+  }();
+  return v;
+}
+
+void chunking(long long n, long long* chunk, int* nchunks) {
+  const long long subs = std::max<long long>(1, (n + FSUB - 1) / FSUB);
+  const long long want = std::max<long long>(1, (long long)sm_count() * 2);
+  const long long per = (subs + want - 1) / want;
+  *chunk = per * FSUB;
+  *nchunks = (int)std::max<long long>(1, (n + *chunk - 1) / *chunk);
+}
+
+struct JaLayout {
+  int* hist_b;
+  int* hist_p;
+  long long* cnt;      // [2B]: build counts, probe counts
+  long long* start;    // [2B]: build starts, probe starts
+  long long* total;    // [2]
+  long long* pkey;
+  int* pgrp;
+  long long* pfk;
+  long long* pval;
+  Slot* table;
+  long long table_slots;
+  long long* reg;      // [2B]: reg_off, reg_cap
+};
+
+JaLayout ja_layout(Arena& a, long long nb, long long np, int B) {
+  JaLayout l{};
+  long long chunk;
+  int nb_ch, np_ch;
+  chunking(nb, &chunk, &nb_ch);
+  chunking(np, &chunk, &np_ch);
+  l.hist_b = a.take<int>((size_t)nb_ch * B);
+  l.hist_p = a.take<int>((size_t)np_ch * B);
+  l.cnt = a.take<long long>(2 * (size_t)B);
+  l.start = a.take<long long>(2 * (size_t)B);
+  l.total = a.take<long long>(2);
+  l.pkey = a.take<long long>(std::max<long long>(nb, 1));
+  l.pgrp = a.take<int>(std::max<long long>(nb, 1));
+  l.pfk = a.take<long long>(std::max<long long>(np, 1));
+  l.pval = a.take<long long>(std::max<long long>(np, 1));
+  l.table_slots = 2 * std::max<long long>(1, std::min(nb, round_rows()));
+  l.table = a.take<Slot>(l.table_slots);
+  l.reg = a.take<long long>(2 * (size_t)B);
+  return l;
+}
+
+struct Round {
+  int p0, p1;            // partitions [p0, p1)
+  long long b_lo, b_hi;  // build rows
+  long long p_lo, p_hi;  // probe rows
+  long long slice_cap;   // > 0: one slice of partition p0
+};
+
+// A thread's pinned staging buffer for the bucket counts.
+long long* pinned_counts(size_t n) {
+  thread_local long long* buf = nullptr;
+  thread_local size_t have = 0;
+  if (have < n) {
+    if (buf) cudaFreeHost(buf);
+    buf = nullptr;
+    have = 0;
+    if (cudaHostAlloc((void**)&buf, n * sizeof(long long), cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    have = n;
+  }
+  return buf;
+}
+
+}  // namespace
+}  // namespace pf
+
+using namespace pf;
+
+extern "C" int pf_join_aggregate_pick_b(int64_t n_build, int64_t n_probe) {
+  (void)n_probe;
+  const long long target = std::max<long long>(1, round_rows() / 2);
+  long long b = 1;
+  while (b < FB_MAX && n_build / b > target) b <<= 1;
+  return (int)b;
+}
+
+extern "C" size_t pf_join_aggregate_workspace(int64_t n_build, int64_t n_probe, int B,
+                                              int64_t n_groups) {
+  (void)n_groups;
+  if (B < 1) B = 1;
+  Arena a(nullptr, 0);
+  ja_layout(a, n_build, n_probe, B);
+  return a.used + 256;
+}
+
+extern "C" int pf_join_aggregate(const int64_t* build_key, const int32_t* build_group,
+                                 int64_t n_build, const int64_t* probe_fk,
+                                 const int64_t* probe_price, const int64_t* probe_disc,
+                                 int64_t scale, int64_t n_probe, int B, int64_t group_min,
+                                 int64_t n_groups, int64_t* sum_out, int64_t* count_out,
+                                 int64_t* stats_out, void* workspace, size_t workspace_bytes,
+                                 void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (B < 1 || B > FB_MAX || (B & (B - 1)))
+    return fail(PF_EINVAL, "join_aggregate: B must be a power of two in [1, %d], got %d", FB_MAX, B);
+  if (n_build < 0 || n_probe < 0 || n_groups < 1 || n_groups > 0xfffffffeLL)
+    return fail(PF_EINVAL, "join_aggregate: bad sizes (build %lld, probe %lld, groups %lld)",
+                (long long)n_build, (long long)n_probe, (long long)n_groups);
+  if (n_build >= (1LL << 40) || n_probe >= (1LL << 40))
+    return fail(PF_EINVAL, "join_aggregate: at most 2^40 rows a side");
+  Arena ar(workspace, workspace_bytes);
+  JaLayout l = ja_layout(ar, n_build, n_probe, B);
+  if (!workspace || !ar.fits())
+    return fail(PF_ENOSPACE, "join_aggregate: workspace of %zu bytes, %zu needed",
+                workspace_bytes, ar.used);
+  const int logB = log2_exact((uint64_t)B);
+  PF_CUDA(cudaMemsetAsync(sum_out, 0, n_groups * sizeof(long long), st));
+  PF_CUDA(cudaMemsetAsync(count_out, 0, n_groups * sizeof(long long), st));
+  PF_CUDA(cudaMemsetAsync(stats_out, 0, 4 * sizeof(long long), st));
+  if (n_build == 0 || n_probe == 0) return ok();
+
+  // 1-2: histograms and offsets of both sides
+  long long chunk_b, chunk_p;
+  int nch_b, nch_p;
+  chunking(n_build, &chunk_b, &nch_b);
+  chunking(n_probe, &chunk_p, &nch_p);
+  const size_t hsm = (size_t)B * sizeof(int);
+  {
+    PF_KERNEL("k_fhist", st);
+    k_fhist<<<nch_b, FT, hsm, st>>>((const long long*)build_key, n_build, chunk_b, logB, B, l.hist_b);
+  }
+  {
+    PF_KERNEL("k_fhist", st);
+    k_fhist<<<nch_p, FT, hsm, st>>>((const long long*)probe_fk, n_probe, chunk_p, logB, B, l.hist_p);
+  }
+  PF_LAUNCH("k_fhist");
+  {
+    PF_KERNEL("k_fscan", st);
+    k_fscan<<<(B + 31) / 32, FT, 0, st>>>(l.hist_b, nch_b, B, l.cnt);
+  }
+  {
+    PF_KERNEL("k_fscan", st);
+    k_fscan<<<(B + 31) / 32, FT, 0, st>>>(l.hist_p, nch_p, B, l.cnt + B);
+  }
+  PF_LAUNCH("k_fscan");
+  PF_CUDA(cudaMemcpyAsync(l.start, l.cnt, 2 * B * sizeof(long long), cudaMemcpyDeviceToDevice, st));
+  {
+    PF_KERNEL("k_scan_counts", st);
+    k_scan_counts<<<1, 1024, 0, st>>>(l.start, B, l.total, nullptr);
+  }
+  {
+    PF_KERNEL("k_scan_counts", st);
+    k_scan_counts<<<1, 1024, 0, st>>>(l.start + B, B, l.total + 1, nullptr);
+  }
+  PF_LAUNCH("k_scan_counts");
+  long long* hc = pinned_counts(2 * (size_t)B);
+  if (!hc) return fail(PF_ECUDA, "join_aggregate: no pinned staging buffer");
+  PF_CUDA(cudaMemcpyAsync(hc, l.cnt, 2 * B * sizeof(long long), cudaMemcpyDeviceToHost, st));
+  cudaEvent_t ev;
+  if (int rc = record_event(st, &ev)) return rc;
+
+  // 3: the scatters, queued while the host waits for the counts
+  const size_t smb = fscatter_smem(B, false), smp = fscatter_smem(B, true);
+  if (int rc = opt_in_smem((const void*)k_fscatter<false>, smb)) return rc;
+  if (int rc = opt_in_smem((const void*)k_fscatter<true>, smp)) return rc;
+  {
+    PF_KERNEL("k_fscatter_build", st);
+    k_fscatter<false><<<nch_b, FT, smb, st>>>((const long long*)build_key, build_group, nullptr, 0,
+                                              n_build, chunk_b, logB, B, l.hist_b, l.start, l.pkey,
+                                              l.pgrp);
+  }
+  {
+    PF_KERNEL("k_fscatter_probe", st);
+    k_fscatter<true><<<nch_p, FT, smp, st>>>((const long long*)probe_fk, probe_price,
+                                             (const long long*)probe_disc, scale, n_probe, chunk_p,
+                                             logB, B, l.hist_p, l.start + B, l.pfk, l.pval);
+  }
+  PF_LAUNCH("k_fscatter");
+  if (int rc = wait_event(ev)) return rc;
+
+  // 4: plan the rounds from the counts
+  const long long cap_rows = l.table_slots / 2;
+  std::vector<Round> rounds;
+  long long bs = 0, ps = 0;
+  for (int p = 0; p < B;) {
+    const long long nbp = hc[p], npp = hc[B + p];
+    if (nbp > cap_rows) {
+      // one partition over the budget: slices of its build rows
+      for (long long s0 = 0; s0 < nbp; s0 += cap_rows) {
+        const long long s1 = std::min(nbp, s0 + cap_rows);
+        rounds.push_back(Round{p, p + 1, bs + s0, bs + s1, ps, ps + npp, 2 * (s1 - s0)});
+      }
+      bs += nbp;
+      ps += npp;
+      ++p;
+      continue;
+    }
+    Round r{p, p, bs, bs, ps, ps, 0};
+    long long rows = 0;
+    while (p < B && hc[p] <= cap_rows && rows + hc[p] <= cap_rows) {
+      rows += hc[p];
+      bs += hc[p];
+      ps += hc[B + p];
+      ++p;
+    }
+    r.p1 = p;
+    r.b_hi = bs;
+    r.p_hi = ps;
+    rounds.push_back(r);
+  }
+  {
+    PF_KERNEL("k_plan", st);
+    k_plan<<<1, 32, 0, st>>>(l.cnt, B, cap_rows, l.reg);
+  }
+  PF_LAUNCH("k_plan");
+  PF_CUDA(cudaMemsetAsync(l.table, 0, l.table_slots * sizeof(Slot), st));
+
+  RoundArgs a{};
+  a.bkey = l.pkey;
+  a.bgrp = l.pgrp;
+  a.pfk = l.pfk;
+  a.pval = l.pval;
+  a.table = l.table;
+  a.reg_off = l.reg;
+  a.reg_cap = l.reg + B;
+  a.logB = logB;
+  a.group_min = group_min;
+  a.n_groups = n_groups;
+  a.sum = (unsigned long long*)sum_out;
+  a.count = (unsigned long long*)count_out;
+  a.stats = (unsigned long long*)stats_out;
+  const int sms = sm_count();
+  for (size_t r = 0; r < rounds.size(); ++r) {
+    const Round& R = rounds[r];
+    a.b_lo = R.b_lo;
+    a.b_hi = R.b_hi;
+    a.p_lo = R.p_lo;
+    a.p_hi = R.p_hi;
+    a.slice_cap = R.slice_cap;
+    a.tag = (unsigned)(r + 1);
+    const long long nbr = R.b_hi - R.b_lo, npr = R.p_hi - R.p_lo;
+    if (nbr > 0) {
+      const unsigned g = (unsigned)std::max<long long>(
+          1, std::min<long long>((nbr + PT2 - 1) / PT2, (long long)sms * 8));
+      {
+        PF_KERNEL("k_fbuild", st);
+        k_fbuild<<<g, PT2, 0, st>>>(a);
+      }
+    }
+    if (nbr > 0 && npr > 0) {
+      const unsigned g = (unsigned)std::max<long long>(
+          1, std::min<long long>((npr + PT2 * PITEMS2 - 1) / (PT2 * PITEMS2), (long long)sms * 8));
+      {
+        PF_KERNEL("k_fprobe", st);
+        k_fprobe<<<g, PT2, 0, st>>>(a);
+      }
+    }
+  }
+  PF_LAUNCH("k_fbuild/k_fprobe");
+  return ok();
+}
+
+namespace {
+struct GfLayout {
+  long long* bcnt;
+  long long* total;
+};
+GfLayout gf_layout(Arena& a, int64_t n) {
+  GfLayout l{};
+  l.bcnt = a.take<long long>((n + CB - 1) / CB + 1);
+  l.total = a.take<long long>(1);
+  return l;
+}
+}  // namespace
+
+extern "C" size_t pf_groups_finish_workspace(int64_t n_groups) {
+  Arena a(nullptr, 0);
+  gf_layout(a, n_groups);
+  return a.used + 256;
+}
+
+extern "C" int pf_groups_finish(const int64_t* sum, const int64_t* count, int64_t group_min,
+                                int64_t n_groups, int64_t* keys_out, int64_t* sums_out,
+                                int64_t* counts_out, int64_t* host_out, void* workspace,
+                                size_t workspace_bytes, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  Arena ar(workspace, workspace_bytes);
+  GfLayout l = gf_layout(ar, n_groups);
+  if (!workspace || !ar.fits())
+    return fail(PF_ENOSPACE, "groups_finish: workspace of %zu bytes, %zu needed", workspace_bytes,
+                ar.used);
+  long long* host_dev = nullptr;
+  if (int rc = host_alias(host_out, (void**)&host_dev)) return rc;
+  if (n_groups <= 0) {
+    host_out[0] = 0;
+    return ok();
+  }
+  const unsigned nblk = blocks_for(n_groups, CB);
+  {
+    PF_KERNEL("k_gcount", st);
+    k_gcount<<<nblk, CT, 0, st>>>((const long long*)count, n_groups, l.bcnt);
+  }
+  PF_LAUNCH("k_gcount");
+  {
+    PF_KERNEL("k_scan_counts", st);
+    k_scan_counts<<<1, 1024, 0, st>>>(l.bcnt, nblk, l.total, host_dev);
+  }
+  PF_LAUNCH("k_scan_counts");
+  cudaEvent_t ev;
+  if (int rc = record_event(st, &ev)) return rc;
+  {
+    PF_KERNEL("k_gemit", st);
+    k_gemit<<<nblk, CT, 0, st>>>((const long long*)sum, (const long long*)count, n_groups,
+                                 group_min, l.bcnt, (long long*)keys_out, (long long*)sums_out,
+                                 (long long*)counts_out);
+  }
+  PF_LAUNCH("k_gemit");
+  if (int rc = wait_event(ev)) return rc;
+  return ok();
+}

@@ -1,0 +1,551 @@
+// The join cores, sm_100a replacements of tqpkernels.join_unique_hash,
+// join_semi_anti and join_expand (reference operators/kernels/join_core.cu,
+// wrapper operators/join_core.py):
+//
+//   unique hash  inner join on a build tuple (1-2 int64 keys) proven unique:
+//                a table of 8-byte slots (build row | 32-bit fingerprint of the
+//                tuple hash), at most half full, linear probing; each probe
+//                row's partner; the matched probe rows compacted in order
+//   semi / anti  a set of the build keys (INT64_MIN marks an empty slot), with
+//                an optional per-key min / max of one build column answering
+//                a residual comparison; the kept probe rows compacted in order
+//   expand       the pairs of the sort/search probe: each probe row's run of
+//                equal build keys, in probe-row order
+//
+// Slots come from the tuple hash's bits just below its top nine (the radix
+// bucket's bits, B <= 512, are shared by a bucket's keys).  Every kernel
+// bounds its probe loop by the table's size.  Each call queues its kernels,
+// writes its row count into the caller's pinned host_out through the device
+// alias, and waits for that count once.
+#include <climits>
+
+#include "scan.cuh"
+
+namespace pf {
+namespace {
+
+constexpr int T = 256;
+constexpr unsigned long long EMPTY_SLOT = ~0ULL;
+constexpr long long EMPTY_KEY = LLONG_MIN;
+
+__device__ __forceinline__ uint64_t tuple_hash(long long k0, long long k1, bool two) {
+  uint64_t h = mix64((uint64_t)k0);
+  if (two) h = mix64(h ^ (mix64((uint64_t)k1) + 0x9e3779b97f4a7c15ULL + (h << 6) + (h >> 2)));
+  return h;
+}
+
+// The first slot of a hash among 2^logcap: the bits right below its top nine.
+__device__ __forceinline__ uint64_t first_slot(uint64_t h, int logcap) {
+  return (h << 9) >> (64 - logcap);
+}
+
+// ---- unique hash -------------------------------------------------------------
+
+template <bool TWO>
+__global__ void __launch_bounds__(T) k_uh_build(const long long* __restrict__ b0,
+                                                const long long* __restrict__ b1, long long n,
+                                                unsigned long long* table, int logcap) {
+  const long long i = (long long)blockIdx.x * T + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t h = tuple_hash(b0[i], TWO ? b1[i] : 0, TWO);
+  const uint64_t mask = (1ULL << logcap) - 1;
+  const unsigned long long entry = ((unsigned long long)(uint32_t)h << 32) | (uint32_t)i;
+  uint64_t s = first_slot(h, logcap);
+  for (uint64_t probes = 0; probes <= mask; ++probes) {
+    if (atomicCAS(&table[s], EMPTY_SLOT, entry) == EMPTY_SLOT) return;
+    s = (s + 1) & mask;
+  }
+}
+
+// Probe CB rows a block: partner[i] (build row or -1), the block's matches.
+template <bool TWO>
+__global__ void __launch_bounds__(CT) k_uh_probe(const long long* __restrict__ b0,
+                                                 const long long* __restrict__ b1,
+                                                 const long long* __restrict__ p0,
+                                                 const long long* __restrict__ p1, long long n,
+                                                 const unsigned long long* __restrict__ table,
+                                                 int logcap, int* __restrict__ partner,
+                                                 long long* __restrict__ bcnt) {
+  const uint64_t mask = (1ULL << logcap) - 1;
+  const long long base = (long long)blockIdx.x * CB;
+  int c = 0;
+#pragma unroll 4
+  for (int k = 0; k < CITEMS; ++k) {
+    const long long i = base + k * CT + threadIdx.x;
+    if (i >= n) break;
+    const long long k0 = p0[i], k1 = TWO ? p1[i] : 0;
+    const uint64_t h = tuple_hash(k0, k1, TWO);
+    const uint32_t fp = (uint32_t)h;
+    uint64_t s = first_slot(h, logcap);
+    int r = -1;
+    for (uint64_t probes = 0; probes <= mask; ++probes) {
+      const unsigned long long e = table[s];
+      if (e == EMPTY_SLOT) break;
+      if ((uint32_t)(e >> 32) == fp) {
+        const int row = (int)(uint32_t)e;
+        if (b0[row] == k0 && (!TWO || b1[row] == k1)) {
+          r = row;
+          break;
+        }
+      }
+      s = (s + 1) & mask;
+    }
+    partner[i] = r;
+    c += r >= 0;
+  }
+  __shared__ int red[CT / 32];
+  for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(FULL, c, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int q = 0; q < CT / 32; ++q) t += red[q];
+    bcnt[blockIdx.x] = t;
+  }
+}
+
+// The matched probe rows of each block, in order, from the block's offset.
+__global__ void __launch_bounds__(CT) k_uh_emit(const int* __restrict__ partner, long long n,
+                                                const long long* __restrict__ boff,
+                                                long long* __restrict__ build_idx,
+                                                long long* __restrict__ probe_idx) {
+  __shared__ int wsum[CT / 32];
+  const long long base = (long long)blockIdx.x * CB + (long long)threadIdx.x * CITEMS;
+  bool keep[CITEMS];
+  int part[CITEMS], rank[CITEMS];
+  if (base + CITEMS <= n) {
+    const int4* v = reinterpret_cast<const int4*>(partner + base);
+#pragma unroll
+    for (int q = 0; q < CITEMS / 4; ++q) {
+      const int4 x = v[q];
+      part[4 * q] = x.x;
+      part[4 * q + 1] = x.y;
+      part[4 * q + 2] = x.z;
+      part[4 * q + 3] = x.w;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < CITEMS; ++k) part[k] = base + k < n ? partner[base + k] : -1;
+  }
+#pragma unroll
+  for (int k = 0; k < CITEMS; ++k) keep[k] = part[k] >= 0;
+  block_ranks(keep, rank, wsum);
+  const long long o = boff[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < CITEMS; ++k) {
+    if (keep[k]) {
+      build_idx[o + rank[k]] = part[k];
+      probe_idx[o + rank[k]] = base + k;
+    }
+  }
+}
+
+// ---- semi / anti ----------------------------------------------------------------
+
+__global__ void __launch_bounds__(T) k_set_build(const long long* __restrict__ key,
+                                                 const long long* __restrict__ val, long long n,
+                                                 long long* table, long long* mn, long long* mx,
+                                                 int logcap, long long* bad) {
+  const long long i = (long long)blockIdx.x * T + threadIdx.x;
+  if (i >= n) return;
+  const long long k = key[i];
+  if (k == EMPTY_KEY) {
+    *bad = 1;
+    return;
+  }
+  const uint64_t mask = (1ULL << logcap) - 1;
+  uint64_t s = first_slot(mix64((uint64_t)k), logcap);
+  bool in = false;
+  for (uint64_t probes = 0; probes <= mask; ++probes) {
+    long long cur = table[s];
+    if (cur == EMPTY_KEY)
+      cur = (long long)atomicCAS((unsigned long long*)&table[s], (unsigned long long)EMPTY_KEY,
+                                 (unsigned long long)k);
+    if (cur == EMPTY_KEY || cur == k) {
+      in = true;
+      break;
+    }
+    s = (s + 1) & mask;
+  }
+  if (!in) {
+    *bad = 2;  // the set is full: cannot happen at half load
+    return;
+  }
+  if (mn || mx) {
+    const long long v = val[i];
+    if (mn && v < mn[s]) atomicMin(&mn[s], v);
+    if (mx && v > mx[s]) atomicMax(&mx[s], v);
+  }
+}
+
+__global__ void __launch_bounds__(CT) k_set_probe(const long long* __restrict__ key,
+                                                  const long long* __restrict__ val, long long n,
+                                                  const long long* __restrict__ table,
+                                                  const long long* __restrict__ mn,
+                                                  const long long* __restrict__ mx, int logcap,
+                                                  int op, bool anti, unsigned char* __restrict__ keep,
+                                                  long long* __restrict__ bcnt) {
+  const uint64_t mask = (1ULL << logcap) - 1;
+  const long long base = (long long)blockIdx.x * CB;
+  int c = 0;
+  for (int k = 0; k < CITEMS; ++k) {
+    const long long i = base + k * CT + threadIdx.x;
+    if (i >= n) break;
+    const long long kk = key[i];
+    bool hit = false;
+    uint64_t s = first_slot(mix64((uint64_t)kk), logcap);
+    if (kk != EMPTY_KEY) {
+      for (uint64_t probes = 0; probes <= mask; ++probes) {
+        const long long t = table[s];
+        if (t == kk) {
+          hit = true;
+          break;
+        }
+        if (t == EMPTY_KEY) break;
+        s = (s + 1) & mask;
+      }
+    }
+    if (hit && op != PF_OP_NONE) {
+      const long long v = val[i];
+      switch (op) {
+        case PF_OP_NE: hit = mn[s] != v || mx[s] != v; break;
+        case PF_OP_LT: hit = mn[s] < v; break;
+        case PF_OP_LE: hit = mn[s] <= v; break;
+        case PF_OP_GT: hit = mx[s] > v; break;
+        default: hit = mx[s] >= v; break;
+      }
+    }
+    const bool kp = hit != anti;
+    keep[i] = kp;
+    c += kp;
+  }
+  __shared__ int red[CT / 32];
+  for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(FULL, c, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int q = 0; q < CT / 32; ++q) t += red[q];
+    bcnt[blockIdx.x] = t;
+  }
+}
+
+__global__ void __launch_bounds__(CT) k_keep_emit(const unsigned char* __restrict__ keep,
+                                                  long long n, const long long* __restrict__ boff,
+                                                  long long* __restrict__ out) {
+  __shared__ int wsum[CT / 32];
+  const long long base = (long long)blockIdx.x * CB + (long long)threadIdx.x * CITEMS;
+  bool kp[CITEMS];
+  int rank[CITEMS];
+  if (base + CITEMS <= n) {
+    const uint4 x = *reinterpret_cast<const uint4*>(keep + base);
+    const unsigned w[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+    for (int k = 0; k < CITEMS; ++k) kp[k] = ((w[k / 4] >> (8 * (k % 4))) & 0xffu) != 0;
+  } else {
+#pragma unroll
+    for (int k = 0; k < CITEMS; ++k) kp[k] = base + k < n && keep[base + k];
+  }
+  block_ranks(kp, rank, wsum);
+  const long long o = boff[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < CITEMS; ++k)
+    if (kp[k]) out[o + rank[k]] = base + k;
+}
+
+__global__ void k_fill_i64(long long* p, long long v, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+// ---- expand ---------------------------------------------------------------------
+
+constexpr int EITEMS = 8;
+
+// Thread t covers pairs [t*EITEMS, t*EITEMS + EITEMS): one binary search for
+// the probe row of its first pair, then a walk.
+__global__ void __launch_bounds__(T) k_expand(const long long* __restrict__ sorted_ids,
+                                              const long long* __restrict__ start,
+                                              const long long* __restrict__ len,
+                                              const long long* __restrict__ incl, long long m,
+                                              long long n_pairs, long long* __restrict__ cs,
+                                              long long* __restrict__ cr) {
+  const long long k0 = ((long long)blockIdx.x * T + threadIdx.x) * EITEMS;
+  if (k0 >= n_pairs) return;
+  long long lo = 0, hi = m - 1;  // first i with incl[i] > k0
+  while (lo < hi) {
+    const long long mid = (lo + hi) >> 1;
+    if (incl[mid] <= k0) lo = mid + 1;
+    else hi = mid;
+  }
+  long long i = lo;
+  long long end = incl[i];
+  for (int e = 0; e < EITEMS; ++e) {
+    const long long k = k0 + e;
+    if (k >= n_pairs) break;
+    while (end <= k && i + 1 < m) end = incl[++i];
+    const long long first = end - len[i];
+    cs[k] = sorted_ids[start[i] + (k - first)];
+    cr[k] = i;
+  }
+}
+
+struct UhLayout {
+  unsigned long long* table;
+  int* partner;
+  long long* bcnt;
+  long long* total;
+};
+
+UhLayout uh_layout(Arena& a, long long nb, long long np) {
+  UhLayout l{};
+  const uint64_t cap = pow2_at_least((uint64_t)std::max<long long>(2 * nb, 2));
+  l.table = a.take<unsigned long long>(cap);
+  l.partner = a.take<int>(std::max<long long>(np, 1));
+  l.bcnt = a.take<long long>((np + CB - 1) / CB + 1);
+  l.total = a.take<long long>(1);
+  return l;
+}
+
+struct SaLayout {
+  long long* table;
+  long long* mn;
+  long long* mx;
+  unsigned char* keep;
+  long long* bcnt;
+  long long* dev;  // [0] kept rows, [1] bad
+};
+
+SaLayout sa_layout(Arena& a, long long nb, long long np, int op) {
+  SaLayout l{};
+  const uint64_t cap = pow2_at_least((uint64_t)std::max<long long>(2 * nb, 2));
+  l.table = a.take<long long>(cap);
+  const bool need_mn = op == PF_OP_NE || op == PF_OP_LT || op == PF_OP_LE;
+  const bool need_mx = op == PF_OP_NE || op == PF_OP_GT || op == PF_OP_GE;
+  l.mn = need_mn ? a.take<long long>(cap) : nullptr;
+  l.mx = need_mx ? a.take<long long>(cap) : nullptr;
+  l.keep = a.take<unsigned char>(std::max<long long>(np, 1));
+  l.bcnt = a.take<long long>((np + CB - 1) / CB + 1);
+  l.dev = a.take<long long>(2);
+  return l;
+}
+
+}  // namespace
+}  // namespace pf
+
+using namespace pf;
+
+extern "C" size_t pf_join_unique_hash_workspace(int64_t n_build, int64_t n_probe) {
+  Arena a(nullptr, 0);
+  uh_layout(a, n_build, n_probe);
+  return a.used + 256;
+}
+
+extern "C" int pf_join_unique_hash(const int64_t* build0, const int64_t* build1, int64_t n_build,
+                                   const int64_t* probe0, const int64_t* probe1, int64_t n_probe,
+                                   int nkeys, int64_t* build_idx, int64_t* probe_idx,
+                                   int64_t* host_out, void* workspace, size_t workspace_bytes,
+                                   void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (nkeys != 1 && nkeys != 2) return fail(PF_EINVAL, "join_unique_hash: one or two keys, got %d", nkeys);
+  if (n_build < 1 || n_probe < 1)
+    return fail(PF_EINVAL, "join_unique_hash: unique hash needs rows on both sides");
+  if (n_build > PF_JOIN_MAX_ROWS || n_probe > PF_JOIN_MAX_ROWS)
+    return fail(PF_EINVAL, "join_unique_hash: a call takes at most %lld rows a side",
+                (long long)PF_JOIN_MAX_ROWS);
+  if (!build0 || !probe0 || (nkeys == 2 && (!build1 || !probe1)) || !build_idx || !probe_idx)
+    return fail(PF_EINVAL, "join_unique_hash: null column");
+  Arena a(workspace, workspace_bytes);
+  UhLayout l = uh_layout(a, n_build, n_probe);
+  if (!workspace || !a.fits())
+    return fail(PF_ENOSPACE, "join_unique_hash: workspace of %zu bytes, %zu needed",
+                workspace_bytes, a.used);
+  long long* host_dev = nullptr;
+  if (int rc = host_alias(host_out, (void**)&host_dev)) return rc;
+  host_out[1] = 0;
+  const uint64_t cap = pow2_at_least((uint64_t)std::max<long long>(2 * n_build, 2));
+  const int logcap = log2_exact(cap);
+  PF_CUDA(cudaMemsetAsync(l.table, 0xff, cap * sizeof(unsigned long long), st));
+  const unsigned nblk = blocks_for(n_probe, CB);
+  const long long* b0 = (const long long*)build0;
+  const long long* b1 = (const long long*)(nkeys == 2 ? build1 : build0);
+  const long long* p0 = (const long long*)probe0;
+  const long long* p1 = (const long long*)(nkeys == 2 ? probe1 : probe0);
+  if (nkeys == 2) {
+    {
+      PF_KERNEL("k_uh_build", 0);
+      k_uh_build<true><<<blocks_for(n_build, T), T, 0, st>>>(b0, b1, n_build, l.table, logcap);
+    }
+    {
+      PF_KERNEL("k_uh_probe", st);
+      k_uh_probe<true><<<nblk, CT, 0, st>>>(b0, b1, p0, p1, n_probe, l.table, logcap, l.partner, l.bcnt);
+    }
+  } else {
+    {
+      PF_KERNEL("k_uh_build", 0);
+      k_uh_build<false><<<blocks_for(n_build, T), T, 0, st>>>(b0, b1, n_build, l.table, logcap);
+    }
+    {
+      PF_KERNEL("k_uh_probe", st);
+      k_uh_probe<false><<<nblk, CT, 0, st>>>(b0, b1, p0, p1, n_probe, l.table, logcap, l.partner, l.bcnt);
+    }
+  }
+  PF_LAUNCH("k_uh_build/k_uh_probe");
+  {
+    PF_KERNEL("k_scan_counts", st);
+    k_scan_counts<<<1, 1024, 0, st>>>(l.bcnt, nblk, l.total, host_dev);
+  }
+  PF_LAUNCH("k_scan_counts");
+  cudaEvent_t ev;
+  if (int rc = record_event(st, &ev)) return rc;
+  {
+    PF_KERNEL("k_uh_emit", st);
+    k_uh_emit<<<nblk, CT, 0, st>>>(l.partner, n_probe, l.bcnt, (long long*)build_idx,
+                                   (long long*)probe_idx);
+  }
+  PF_LAUNCH("k_uh_emit");
+  if (int rc = wait_event(ev)) return rc;
+  return ok();
+}
+
+extern "C" size_t pf_join_semi_anti_workspace(int64_t n_build, int64_t n_probe, int op) {
+  Arena a(nullptr, 0);
+  sa_layout(a, n_build, n_probe, op);
+  return a.used + 256;
+}
+
+extern "C" int pf_join_semi_anti(const int64_t* build_key, int64_t n_build,
+                                 const int64_t* probe_key, int64_t n_probe,
+                                 const int64_t* build_val, const int64_t* probe_val, int op,
+                                 int anti, int64_t* out, int64_t* host_out, void* workspace,
+                                 size_t workspace_bytes, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (n_build < 1 || n_probe < 1)
+    return fail(PF_EINVAL, "join_semi_anti: semi/anti needs rows on both sides");
+  if (n_probe > PF_JOIN_MAX_ROWS || n_build > PF_JOIN_MAX_ROWS)
+    return fail(PF_EINVAL, "join_semi_anti: a call takes at most %lld rows a side",
+                (long long)PF_JOIN_MAX_ROWS);
+  if (op < PF_OP_NONE || op > PF_OP_GE) return fail(PF_EINVAL, "join_semi_anti: unknown residual operator %d", op);
+  if (op != PF_OP_NONE && (!build_val || !probe_val))
+    return fail(PF_EINVAL, "join_semi_anti: a residual needs both value columns");
+  Arena a(workspace, workspace_bytes);
+  SaLayout l = sa_layout(a, n_build, n_probe, op);
+  if (!workspace || !a.fits())
+    return fail(PF_ENOSPACE, "join_semi_anti: workspace of %zu bytes, %zu needed", workspace_bytes,
+                a.used);
+  long long* host_dev = nullptr;
+  if (int rc = host_alias(host_out, (void**)&host_dev)) return rc;
+  const uint64_t cap = pow2_at_least((uint64_t)std::max<long long>(2 * n_build, 2));
+  const int logcap = log2_exact(cap);
+  const unsigned fill_blocks = (unsigned)std::min<uint64_t>((cap + 255) / 256, 4096);
+  {
+    PF_KERNEL("k_fill_i64", st);
+    k_fill_i64<<<fill_blocks, 256, 0, st>>>(l.table, EMPTY_KEY, (long long)cap);
+  }
+  if (l.mn) k_fill_i64<<<fill_blocks, 256, 0, st>>>(l.mn, LLONG_MAX, (long long)cap);
+  if (l.mx) k_fill_i64<<<fill_blocks, 256, 0, st>>>(l.mx, LLONG_MIN, (long long)cap);
+  host_out[0] = 0;
+  host_out[1] = 0;  // the build below sets it through the alias
+  {
+    PF_KERNEL("k_set_build", 0);
+    k_set_build<<<blocks_for(n_build, T), T, 0, st>>>((const long long*)build_key,
+                                                      (const long long*)build_val, n_build, l.table,
+                                                      l.mn, l.mx, logcap, host_dev + 1);
+  }
+  PF_LAUNCH("k_set_build");
+  const unsigned nblk = blocks_for(n_probe, CB);
+  {
+    PF_KERNEL("k_set_probe", st);
+    k_set_probe<<<nblk, CT, 0, st>>>((const long long*)probe_key, (const long long*)probe_val,
+                                     n_probe, l.table, l.mn, l.mx, logcap, op, anti != 0, l.keep,
+                                     l.bcnt);
+  }
+  PF_LAUNCH("k_set_probe");
+  {
+    PF_KERNEL("k_scan_counts", st);
+    k_scan_counts<<<1, 1024, 0, st>>>(l.bcnt, nblk, l.dev, host_dev);
+  }
+  PF_LAUNCH("k_scan_counts");
+  cudaEvent_t ev;
+  if (int rc = record_event(st, &ev)) return rc;
+  {
+    PF_KERNEL("k_keep_emit", st);
+    k_keep_emit<<<nblk, CT, 0, st>>>(l.keep, n_probe, l.bcnt, (long long*)out);
+  }
+  PF_LAUNCH("k_keep_emit");
+  if (int rc = wait_event(ev)) return rc;
+  if (host_out[1] == 2) return fail(PF_EDEVICE, "join_semi_anti: the key set overflowed");
+  return ok();
+}
+
+extern "C" size_t pf_join_expand_workspace(int64_t m) {
+  Arena a(nullptr, 0);
+  a.take<long long>(std::max<int64_t>(m, 1));           // incl
+  a.take<long long>(1);                                 // total
+  a.take<long long>(scan_scratch_elems(std::max<int64_t>(m, 1)));
+  return a.used + 256;
+}
+
+namespace {
+struct ExLayout {
+  long long* incl;
+  long long* total;
+  long long* scratch;
+};
+ExLayout ex_layout(Arena& a, int64_t m) {
+  ExLayout l{};
+  l.incl = a.take<long long>(std::max<int64_t>(m, 1));
+  l.total = a.take<long long>(1);
+  l.scratch = a.take<long long>(scan_scratch_elems(std::max<int64_t>(m, 1)));
+  return l;
+}
+}  // namespace
+
+extern "C" int pf_join_expand_prepare(const int64_t* len, int64_t m, int64_t* host_out,
+                                      void* workspace, size_t workspace_bytes, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (m < 0 || m > PF_JOIN_MAX_ROWS)
+    return fail(PF_EINVAL, "join_expand: at most %lld probe rows", (long long)PF_JOIN_MAX_ROWS);
+  Arena a(workspace, workspace_bytes);
+  ExLayout l = ex_layout(a, m);
+  if (!workspace || !a.fits())
+    return fail(PF_ENOSPACE, "join_expand: workspace of %zu bytes, %zu needed", workspace_bytes,
+                a.used);
+  long long* host_dev = nullptr;
+  if (int rc = host_alias(host_out, (void**)&host_dev)) return rc;
+  if (m == 0) {
+    host_out[0] = 0;
+    return ok();
+  }
+  if (int rc = scan_i64((const long long*)len, l.incl, m, true, l.total, l.scratch, st)) return rc;
+  {
+    PF_KERNEL("k_copy_i64", st);
+    k_copy_i64<<<1, 32, 0, st>>>(l.total, host_dev, 1);
+  }
+  PF_LAUNCH("k_copy_i64");
+  if (int rc = wait_stream(st)) return rc;
+  return ok();
+}
+
+extern "C" int pf_join_expand(const int64_t* sorted_ids, const int64_t* start, const int64_t* len,
+                              int64_t m, int64_t n_pairs, int64_t* cs, int64_t* cr,
+                              void* workspace, size_t workspace_bytes, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (n_pairs <= 0 || m <= 0) return ok();
+  Arena a(workspace, workspace_bytes);
+  ExLayout l = ex_layout(a, m);
+  if (!workspace || !a.fits())
+    return fail(PF_ENOSPACE, "join_expand: workspace of %zu bytes, %zu needed", workspace_bytes,
+                a.used);
+  const long long threads = (n_pairs + EITEMS - 1) / EITEMS;
+  {
+    PF_KERNEL("k_expand", 0);
+    k_expand<<<blocks_for(threads, T), T, 0, st>>>((const long long*)sorted_ids,
+                                                   (const long long*)start, (const long long*)len,
+                                                   l.incl, m, n_pairs, (long long*)cs,
+                                                   (long long*)cr);
+  }
+  PF_LAUNCH("k_expand");
+  return ok();
+}

@@ -1,0 +1,116 @@
+"""The fused join -> group-by on sm_100a (pf_join_aggregate): radix partition
+of both sides, per-round L2-resident hash tables, probe rows aggregated
+straight into a dense group slab, then the occupied groups compacted.
+
+    keys, sums, counts = join_group_aggregate(build_key, build_group,
+                                              probe_fk, price, disc)
+
+computes ``SELECT group, SUM(price * (scale - disc)), COUNT(*) FROM build
+JOIN probe ON build.key = probe.fk GROUP BY group`` for a unique build key:
+the result the reference produces by partition_sort -> join_unique_hash ->
+index_select -> KeyedAggregate.pass1 -> reduce_tick_slice (uvm/join.py,
+uvm/aggregate.py), with exact int64 sums.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import Optional
+
+import torch
+
+from . import _native as N
+
+
+@dataclass
+class JoinAggregateStats:
+    matched: int          # probe rows that found their build row
+    bad_groups: int       # build rows whose group lay outside the range
+    overflow: int         # build rows no table slot took (0 unless broken)
+
+
+class JoinAggregate:
+    """A reusable plan for one input shape: its workspace and output slabs
+    are allocated once, so repeated ``run`` calls allocate nothing (and the
+    queued work can be timed or captured as is)."""
+
+    def __init__(self, n_build: int, n_probe: int, group_min: int, n_groups: int,
+                 device, B: Optional[int] = None, scale: int = 100):
+        self.n_build, self.n_probe = int(n_build), int(n_probe)
+        self.group_min, self.n_groups = int(group_min), int(n_groups)
+        self.scale = int(scale)
+        self.device = torch.device(device)
+        L = N.lib()
+        self.B = int(B) if B else int(L.pf_join_aggregate_pick_b(self.n_build, self.n_probe))
+        self.ws_bytes = int(L.pf_join_aggregate_workspace(self.n_build, self.n_probe, self.B,
+                                                          self.n_groups))
+        self.ws = N.workspace(self.ws_bytes, self.device)
+        self.sum = torch.empty(self.n_groups, dtype=torch.int64, device=self.device)
+        self.count = torch.empty(self.n_groups, dtype=torch.int64, device=self.device)
+        self.stats = torch.zeros(4, dtype=torch.int64, device=self.device)
+        self.keys_out = torch.empty(self.n_groups, dtype=torch.int64, device=self.device)
+        self.sums_out = torch.empty(self.n_groups, dtype=torch.int64, device=self.device)
+        self.counts_out = torch.empty(self.n_groups, dtype=torch.int64, device=self.device)
+        self.fin_bytes = int(L.pf_groups_finish_workspace(self.n_groups))
+        self.fin_ws = N.workspace(self.fin_bytes, self.device)
+        self.host = torch.zeros(2, dtype=torch.int64, pin_memory=True)
+
+    def aggregate(self, build_key, build_group, probe_fk, probe_price, probe_disc=None):
+        """Queues the join + dense aggregation into ``self.sum`` /
+        ``self.count`` (waits once, for the bucket counts)."""
+        for t, n, dt, name in ((build_key, self.n_build, torch.int64, "build_key"),
+                               (build_group, self.n_build, torch.int32, "build_group"),
+                               (probe_fk, self.n_probe, torch.int64, "probe_fk"),
+                               (probe_price, self.n_probe, torch.int64, "probe_price")):
+            if not (t.is_cuda and t.dtype == dt and t.dim() == 1 and t.numel() == n
+                    and t.is_contiguous()):
+                raise ValueError(f"{name} must be a contiguous 1-D {dt} CUDA tensor of {n} rows")
+        if probe_disc is not None and not (probe_disc.is_cuda and probe_disc.dtype == torch.int64
+                                           and probe_disc.numel() == self.n_probe
+                                           and probe_disc.is_contiguous()):
+            raise ValueError("probe_disc must match probe_fk")
+        L = N.lib()
+        with torch.cuda.device(self.device):
+            rc = L.pf_join_aggregate(
+                build_key.data_ptr(), build_group.data_ptr(), self.n_build,
+                probe_fk.data_ptr(), probe_price.data_ptr(), N.ptr(probe_disc), self.scale,
+                self.n_probe, self.B, self.group_min, self.n_groups, self.sum.data_ptr(),
+                self.count.data_ptr(), self.stats.data_ptr(), self.ws.data_ptr(),
+                self.ws_bytes, N.stream_of(self.device))
+        N.check(rc, "join_aggregate")
+
+    def finish(self):
+        """The occupied groups, ascending: (keys, sums, counts)."""
+        L = N.lib()
+        with torch.cuda.device(self.device):
+            rc = L.pf_groups_finish(self.sum.data_ptr(), self.count.data_ptr(), self.group_min,
+                                    self.n_groups, self.keys_out.data_ptr(),
+                                    self.sums_out.data_ptr(), self.counts_out.data_ptr(),
+                                    self.host.data_ptr(), self.fin_ws.data_ptr(),
+                                    self.fin_bytes, N.stream_of(self.device))
+        N.check(rc, "groups_finish")
+        n = int(self.host[0])
+        return self.keys_out[:n], self.sums_out[:n], self.counts_out[:n]
+
+    def run(self, build_key, build_group, probe_fk, probe_price, probe_disc=None):
+        self.aggregate(build_key, build_group, probe_fk, probe_price, probe_disc)
+        return self.finish()
+
+    def read_stats(self) -> JoinAggregateStats:
+        s = self.stats.tolist()
+        return JoinAggregateStats(matched=s[0], bad_groups=s[2], overflow=s[3])
+
+
+def join_group_aggregate(build_key, build_group, probe_fk, probe_price, probe_disc=None,
+                         scale: int = 100, group_min: Optional[int] = None,
+                         n_groups: Optional[int] = None, B: Optional[int] = None):
+    """One-shot form: (group keys ascending, int64 sums, int64 counts).  The
+    group range defaults to the build groups' [min, max] (one host read)."""
+    if group_min is None or n_groups is None:
+        if build_group.numel() == 0:
+            e = torch.empty(0, dtype=torch.int64, device=build_key.device)
+            return e, e.clone(), e.clone()
+        lo, hi = torch.aminmax(build_group)
+        group_min, n_groups = int(lo), int(hi) - int(lo) + 1
+    plan = JoinAggregate(build_key.numel(), probe_fk.numel(), group_min, n_groups,
+                         build_key.device, B=B, scale=scale)
+    return plan.run(build_key, build_group, probe_fk, probe_price, probe_disc)

@@ -1,0 +1,226 @@
+"""The slab group-by and the fused join -> group-by on the GPU:
+
+* DenseAggregationSlab (pf_slab_add / pf_slab_finish) against the vectors the
+  reference's own DenseAggregationSlab produced (tests/golden/slab.json), and
+  its feed-chunking invariance and identities (the reference's
+  tests/aggregate_merge/test_aggregation_slab.py cases);
+* the fused join + group-by (pf_join_aggregate) against the small workload's
+  golden result from the reference's operators, against the oracle on random
+  inputs (every fan-out, slices of a partition over the table budget, empty
+  and ragged inputs, groups out of range, negative and extreme keys), and the
+  device generator against the CPU one.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from pageflow_b200 import datagen
+from pageflow_b200.aggregation_slab import DenseAggregationSlab
+from pageflow_b200.join_aggregate import JoinAggregate, join_group_aggregate
+from tests.golden import load
+
+pytestmark = pytest.mark.gpu
+
+
+# ---- slab -------------------------------------------------------------------------
+
+@pytest.mark.parametrize("case", range(4))
+def test_slab_matches_the_references_vectors(case):
+    g = load("slab.json")[case]
+    specs = [(torch.int64, ()), (torch.int64, ()), (torch.int64, ()), (torch.float64, (2,))]
+    s = DenseAggregationSlab(g["lo"], g["hi"], torch.int64, specs, g["ops"], "cuda")
+    for k, v1, v2, v3, v4 in g["ticks"]:
+        s.add(torch.tensor(k, device="cuda"),
+              [torch.tensor(v1, device="cuda"), torch.tensor(v2, device="cuda"),
+               torch.tensor(v3, device="cuda"),
+               torch.tensor(v4, dtype=torch.float64, device="cuda")])
+    keys, vals = s.finish()
+    assert keys.tolist() == g["keys"]
+    for got, want in zip(vals, g["vals"]):
+        # integer values bit-exact; the float sums hold small integers, exact too
+        assert got.tolist() == want
+
+
+def test_feed_chunking_does_not_change_slab_result():
+    keys = torch.tensor([4, 2, 4, 7, 2, 4, 7, 3], device="cuda")
+    states = torch.tensor([[1.0, 1.0], [2.0, 1.0], [3.0, 1.0], [4.0, 1.0], [5.0, 1.0],
+                           [6.0, 1.0], [7.0, 1.0], [8.0, 1.0]], dtype=torch.float64,
+                          device="cuda")
+    one = DenseAggregationSlab(2, 7, torch.int64, [(torch.float64, (2,))], ["sum"], "cuda")
+    one.add(keys, [states])
+    many = DenseAggregationSlab(2, 7, torch.int64, [(torch.float64, (2,))], ["sum"], "cuda")
+    for lo, hi in ((0, 1), (1, 5), (5, 6), (6, 8)):
+        many.add(keys[lo:hi], [states[lo:hi]])
+    ka, va = one.finish()
+    kb, vb = many.finish()
+    assert torch.equal(ka, kb) and torch.equal(va[0], vb[0])
+    assert ka.tolist() == [2, 3, 4, 7]
+    assert va[0].tolist() == [[7.0, 2.0], [8.0, 1.0], [10.0, 3.0], [11.0, 2.0]]
+
+
+def test_amax_and_amin_identities_do_not_poison_first_value():
+    s = DenseAggregationSlab(10, 12, torch.int64, [(torch.int64, ()), (torch.int64, ())],
+                             ["amax", "amin"], "cuda")
+    s.add(torch.tensor([10, 10, 12], device="cuda"),
+          [torch.tensor([-8, -3, -11], device="cuda"), torch.tensor([8, 3, 11], device="cuda")])
+    keys, values = s.finish()
+    assert keys.tolist() == [10, 12]
+    assert values[0].tolist() == [-3, -11] and values[1].tolist() == [3, 11]
+
+
+def test_slab_large_sum_is_exact_int64():
+    n, G = 5_000_000, 100_003
+    g = torch.Generator().manual_seed(9)
+    keys = torch.randint(0, G, (n,), generator=g)
+    vals = torch.randint(-(1 << 40), 1 << 40, (n,), generator=g)
+    s = DenseAggregationSlab(0, G - 1, torch.int64, [(torch.int64, ())], ["sum"], "cuda")
+    s.add(keys.cuda(), [vals.cuda()])
+    k, (v,) = s.finish()
+    want = np.zeros(G, np.int64)
+    np.add.at(want, keys.numpy(), vals.numpy())
+    present = np.unique(keys.numpy())
+    assert np.array_equal(k.cpu().numpy(), present)
+    assert np.array_equal(v.cpu().numpy(), want[present])
+
+
+# ---- the fused join -> group-by ---------------------------------------------------
+
+def _oracle_groups(bkey, bgrp, fk, price, disc, group_min, n_groups, scale=100):
+    s, c, matched, _ = oracle.join_aggregate(
+        bkey.cpu().numpy(), bgrp.cpu().numpy(), fk.cpu().numpy(), price.cpu().numpy(),
+        disc.cpu().numpy() if disc is not None else None, scale, group_min, n_groups, B=16)
+    present = np.nonzero(c)[0]
+    return group_min + present, s[present], c[present], matched
+
+
+def _assert_groups(got, want):
+    keys, sums, counts = got
+    assert np.array_equal(keys.cpu().numpy(), want[0])
+    assert np.array_equal(sums.cpu().numpy(), want[1])
+    assert np.array_equal(counts.cpu().numpy(), want[2])
+
+
+def test_small_workload_is_the_references_result():
+    """250K x 1M, seed 0: the groups, sums and counts of the reference's
+    join + KeyedAggregate.pass1 + reduce_tick_slice."""
+    g = load("config0.npz")
+    w = datagen.SMALL
+    bkey, bgrp = datagen.gen_build(w, "cuda")
+    fk, price, disc = datagen.gen_probe(w, "cuda")
+    plan = JoinAggregate(w.n_build, w.n_probe, 0, w.n_groups, "cuda")
+    keys, sums, counts = plan.run(bkey, bgrp, fk, price, disc)
+    assert np.array_equal(keys.cpu().numpy(), g["groups"])
+    assert np.array_equal(sums.cpu().numpy(), g["sums"])
+    assert np.array_equal(counts.cpu().numpy(), g["counts"])
+    st = plan.read_stats()
+    assert st.matched == int(g["matched"][0]) and st.overflow == 0 and st.bad_groups == 0
+
+
+def test_device_generator_is_the_cpu_generator():
+    w = datagen.scaled(datagen.SCALE, 1 / 1000)
+    bkey, bgrp = datagen.gen_build(w, "cuda", lo=17, rows=50_000)
+    fk, price, disc = datagen.gen_probe(w, "cuda", lo=123_456, rows=200_000)
+    obk, obg = oracle.gen_build(w.seed, w.n_build, w.n_groups, 17, 50_000)
+    ofk, opr, odi = oracle.gen_probe(w.config, w.seed, w.n_build, 123_456, 200_000)
+    assert np.array_equal(bkey.cpu().numpy(), obk) and np.array_equal(bgrp.cpu().numpy(), obg)
+    assert np.array_equal(fk.cpu().numpy(), ofk)
+    assert np.array_equal(price.cpu().numpy(), opr)
+    assert np.array_equal(disc.cpu().numpy(), odi)
+
+
+@pytest.mark.parametrize("B", [1, 2, 16, 64, 256, 512, 1024, 4096])
+def test_every_fan_out_matches_the_oracle(B):
+    w = datagen.scaled(datagen.SCALE, 1 / 500)   # 300K x 1.2M, 3000 groups
+    bkey, bgrp = datagen.gen_build(w, "cuda")
+    fk, price, disc = datagen.gen_probe(w, "cuda")
+    want = _oracle_groups(bkey, bgrp, fk, price, disc, 0, w.n_groups)
+    plan = JoinAggregate(w.n_build, w.n_probe, 0, w.n_groups, "cuda", B=B)
+    _assert_groups(plan.run(bkey, bgrp, fk, price, disc), want)
+    st = plan.read_stats()
+    assert st.matched == want[3] and st.overflow == 0
+
+
+def test_partitions_over_the_table_budget_take_slices(monkeypatch):
+    """B = 1 over 3M build rows: one partition over the 1.5M-row table
+    budget, joined in slices, each probe row meeting every slice."""
+    w = datagen.scaled(datagen.SCALE, 1 / 50)   # 3M x 12M
+    bkey, bgrp = datagen.gen_build(w, "cuda")
+    fk, price, disc = datagen.gen_probe(w, "cuda")
+    want = _oracle_groups(bkey, bgrp, fk, price, disc, 0, w.n_groups)
+    for B in (1, 2):
+        plan = JoinAggregate(w.n_build, w.n_probe, 0, w.n_groups, "cuda", B=B)
+        _assert_groups(plan.run(bkey, bgrp, fk, price, disc), want)
+        assert plan.read_stats().matched == want[3]
+
+
+def _random_case(nb, np_, G, seed, gmin=0):
+    g = torch.Generator().manual_seed(seed)
+    bkey = (torch.randperm(max(4 * nb, 1), generator=g)[:nb].to(torch.int64) * 104729
+            - (1 << 50))
+    bgrp = torch.randint(gmin, gmin + G, (nb,), generator=g, dtype=torch.int32)
+    if nb:
+        fk = bkey[torch.randint(0, nb, (np_,), generator=g)]
+        fk = torch.where(torch.rand(np_, generator=g) < 0.2, fk + 1, fk)
+    else:
+        fk = torch.randint(-100, 100, (np_,), generator=g)
+    price = torch.randint(-(1 << 30), 1 << 30, (np_,), generator=g)
+    disc = torch.randint(0, 11, (np_,), generator=g)
+    return [t.cuda() for t in (bkey, bgrp, fk, price, disc)]
+
+
+@pytest.mark.parametrize("nb,np_,G", [(0, 10, 5), (10, 0, 5), (1, 1, 1), (3, 4097, 2),
+                                      (4097, 3, 7), (50_000, 200_003, 1),
+                                      (123_457, 654_321, 50_000)])
+def test_ragged_and_empty_inputs(nb, np_, G):
+    bkey, bgrp, fk, price, disc = _random_case(nb, np_, G, nb + np_, gmin=-3)
+    want = _oracle_groups(bkey, bgrp, fk, price, disc, -3, G)
+    got = join_group_aggregate(bkey, bgrp, fk, price, disc, group_min=-3, n_groups=G, B=32)
+    _assert_groups(got, want)
+
+
+def test_no_discount_column_and_another_scale():
+    bkey, bgrp, fk, price, disc = _random_case(20_000, 90_000, 100, 5)
+    want = _oracle_groups(bkey, bgrp, fk, price, None, 0, 100)
+    _assert_groups(join_group_aggregate(bkey, bgrp, fk, price, None, group_min=0, n_groups=100),
+                   want)
+    want = _oracle_groups(bkey, bgrp, fk, price, disc, 0, 100, scale=7)
+    _assert_groups(join_group_aggregate(bkey, bgrp, fk, price, disc, scale=7, group_min=0,
+                                        n_groups=100), want)
+
+
+def test_groups_outside_the_range_are_counted_not_aggregated():
+    bkey, bgrp, fk, price, disc = _random_case(10_000, 40_000, 50, 6)
+    plan = JoinAggregate(10_000, 40_000, 10, 20, "cuda", B=8)   # groups [10, 30) only
+    keys, sums, counts = plan.run(bkey, bgrp, fk, price, disc)
+    want = _oracle_groups(bkey, bgrp, fk, price, disc, 10, 20)
+    _assert_groups((keys, sums, counts), want)
+    st = plan.read_stats()
+    assert st.bad_groups == int(((bgrp < 10) | (bgrp >= 30)).sum())
+
+
+def test_repeated_runs_of_one_plan_are_identical():
+    w = datagen.scaled(datagen.SCALE, 1 / 1000)
+    bkey, bgrp = datagen.gen_build(w, "cuda")
+    fk, price, disc = datagen.gen_probe(w, "cuda")
+    plan = JoinAggregate(w.n_build, w.n_probe, 0, w.n_groups, "cuda")
+    first = [t.clone() for t in plan.run(bkey, bgrp, fk, price, disc)]
+    for _ in range(3):
+        for a, b in zip(first, plan.run(bkey, bgrp, fk, price, disc)):
+            assert torch.equal(a, b)
+
+
+def test_scale_workload_tenth_matches_the_generator_expectation():
+    """A tenth of the 150M x 600M workload (15M x 60M, 150K groups) against
+    the exact expectation from the generator (every group's sum and count)."""
+    w = datagen.scaled(datagen.SCALE, 1 / 10)
+    bkey, bgrp = datagen.gen_build(w, "cuda")
+    fk, price, disc = datagen.gen_probe(w, "cuda")
+    plan = JoinAggregate(w.n_build, w.n_probe, 0, w.n_groups, "cuda")
+    plan.aggregate(bkey, bgrp, fk, price, disc)
+    s, c, m = oracle.expected_groups(w.config, w.seed, w.n_build, w.n_groups, 0, w.n_probe)
+    assert np.array_equal(plan.sum.cpu().numpy(), s)
+    assert np.array_equal(plan.count.cpu().numpy(), c)
+    assert plan.read_stats().matched == m

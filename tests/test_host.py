@@ -1,0 +1,168 @@
+"""CPU tests of the host side: the C-ABI library loads and exports every
+function include/pageflow_b200.h declares (no GPU work is started), the
+argument checks that run before any kernel, the partition-count rule against
+the reference's own values, and the operator mirrors' validation."""
+from __future__ import annotations
+
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+import torch
+
+from tests.golden import load
+
+REPO = Path(__file__).resolve().parents[1]
+
+
+def header_functions():
+    text = (REPO / "include" / "pageflow_b200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(pf_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_function():
+    from pageflow_b200 import _native
+    L = _native.lib()
+    declared = header_functions()
+    assert len(declared) >= 20
+    for name in declared:
+        assert hasattr(L, name), name
+    # and the Python binding covers each of them
+    assert sorted(_native.exported_symbols()) == declared
+
+
+def test_library_is_the_in_tree_build():
+    from pageflow_b200 import _native
+    assert _native.LIB_PATH.parent == REPO / "pageflow_b200"
+    assert _native.lib().pf_version().decode() == "0.1.0"
+
+
+def test_rows_per_unit_is_lcm_over_row_bytes():
+    from pageflow_b200 import _native
+    L = _native.lib()
+    for rb in (1, 2, 3, 4, 8, 16, 25, 24, 512, 1000):
+        import math
+        assert L.pf_rows_per_unit(rb) == math.lcm(rb, 512) // rb
+
+
+def test_workspace_sizes_are_host_arithmetic():
+    from pageflow_b200 import _native
+    L = _native.lib()
+    a = L.pf_partition_sort_workspace(1 << 20, 1 << 20, 64, 0, 0)
+    b = L.pf_partition_sort_workspace(1 << 24, 1 << 24, 512, 1, 1)
+    assert 0 < a < b
+    assert L.pf_join_unique_hash_workspace(1000, 2000) >= 2048 * 8 + 2000 * 4
+    assert L.pf_join_aggregate_workspace(1000, 4000, 1, 25) >= 1000 * 12 + 4000 * 16
+    assert L.pf_join_aggregate_pick_b(250_000, 1_000_000) == 1
+    assert 256 <= L.pf_join_aggregate_pick_b(150_000_000, 600_000_000) <= 4096
+
+
+def test_invalid_arguments_fail_before_any_kernel():
+    """Argument checks return PF_EINVAL with a message and touch no GPU."""
+    from pageflow_b200 import _native
+    L = _native.lib()
+    rc = L.pf_partition_sort(None, None, None, None, 0, 0, None, 10, 10, 0, 32, 0, None, None,
+                             None, 0, None)
+    assert rc == _native.PF_EINVAL
+    assert "columns" in L.pf_last_error().decode()
+    ptrs = (ctypes.c_void_p * 1)(1)
+    rb = (ctypes.c_int * 1)(8)
+    comp = (ctypes.c_int * 1)(0)
+    rc = L.pf_partition_sort(ptrs, ptrs, rb, comp, 1, 0, None, 10, 10, 0, 24, 0, 1, 1, None,
+                             0, None)
+    assert rc == _native.PF_EINVAL and "power of two" in L.pf_last_error().decode()
+    rc = L.pf_join_unique_hash(1, None, 0, 1, None, 5, 1, 1, 1, 1, None, 0, None)
+    assert rc == _native.PF_EINVAL and "both sides" in L.pf_last_error().decode()
+    rc = L.pf_join_aggregate(1, 1, 10, 1, 1, None, 100, 10, 24, 0, 5, 1, 1, 1, None, 0, None)
+    assert rc == _native.PF_EINVAL and "power of two" in L.pf_last_error().decode()
+
+
+def test_partition_count_rule_is_the_references():
+    from pageflow_b200 import partitions
+    g = load("partitions.json")
+    assert partitions.JOIN_B_MAX == g["JOIN_B_MAX"]
+    assert partitions.AGG_B_MAX == g["AGG_B_MAX"]
+    for m, n, want in g["max_load"]:
+        assert partitions.max_load(m, n) == pytest.approx(want, rel=1e-12, abs=0)
+    for parts, budget, bmax, want in g["partition_count"]:
+        got = partitions.partition_count([tuple(p) for p in parts], budget, bmax)
+        assert got[0] == want[0]
+        assert got[1] == pytest.approx(want[1], rel=1e-12)
+    for args, want in g["agg_partitions"]:
+        got = partitions.agg_partitions(*args)
+        assert got[0] == want[0] and got[2] == want[2]
+        assert got[1] == pytest.approx(want[1], rel=1e-12)
+
+
+def test_bucket_limit_is_the_join_cap():
+    from pageflow_b200 import partition_sort, partitions, tqpkernels
+    assert partition_sort._B_MAX == partitions.JOIN_B_MAX == tqpkernels.BMAX
+    h = (REPO / "include" / "pageflow_b200.h").read_text()
+    assert re.search(r"#define PF_PART_B_MAX (\d+)", h).group(1) == str(partitions.JOIN_B_MAX)
+
+
+@pytest.mark.parametrize("case", ["five widths", "seven columns", "int32 key", "B=1024",
+                                  "B=24", "B=0"])
+def test_ticks_outside_the_limits_raise(case):
+    """The mirror's limits, checked before any kernel (CPU tensors suffice)."""
+    from pageflow_b200.partition_sort import partition
+    n = 1000
+    key = torch.arange(n, dtype=torch.int64)
+    cols, B = {
+        "five widths": ([key, key.to(torch.int32), key.to(torch.int16), key.to(torch.int8),
+                         torch.zeros(n, 25, dtype=torch.uint8)], 32),
+        "seven columns": ([key] * 7, 32),
+        "int32 key": ([key.to(torch.int32)], 32),
+        "B=1024": ([key], 1024),
+        "B=24": ([key], 24),
+        "B=0": ([key], 0),
+    }[case]
+    with pytest.raises(ValueError, match="outside the kernel's limits"):
+        partition(cols, 0, None, 0, B)
+
+
+def test_raw_columns_without_the_count_raise():
+    from pageflow_b200.partition_sort import partition
+    key = torch.arange(100, dtype=torch.int64)
+    mask = torch.ones(100, dtype=torch.bool)
+    with pytest.raises(ValueError, match="need the mask's kept rows"):
+        partition([key], 0, mask, 0, 16)
+
+
+def test_a_count_the_compacted_rows_contradict_raises():
+    from pageflow_b200.partition_sort import partition
+    key = torch.arange(50, dtype=torch.int64)
+    mask = torch.zeros(100, dtype=torch.bool)
+    mask[::2] = True
+    with pytest.raises(RuntimeError, match="compacted columns hold"):
+        partition([key], 0, mask, 0, 32, n_valid=51)
+
+
+def test_join_core_validation_runs_before_the_kernel():
+    from pageflow_b200 import join_core
+    k = torch.arange(4, dtype=torch.int64)
+    with pytest.raises(ValueError, match="1-D CUDA int64"):
+        join_core.unique_hash_pairs([k], [k])
+    with pytest.raises(ValueError, match="one or two"):
+        join_core.unique_hash_pairs([k, k, k], [k, k, k])
+
+
+def test_padded_layout_matches_the_oracle():
+    import oracle
+    from pageflow_b200.partition_sort import aligned_partition_layout
+    counts = [0, 5, 130, 1, 0, 64]
+    for rb in (1, 4, 8, 25):
+        unit = rb * 512 // __import__("math").gcd(rb, 512)
+        _, starts_b, total = aligned_partition_layout(counts, rb, unit)
+        starts, total2 = oracle.padded_layout(counts, rb)
+        assert [s // rb for s in starts_b] == starts and total == total2
+
+
+def test_slab_rejects_bad_specs_on_the_host():
+    from pageflow_b200.aggregation_slab import DenseAggregationSlab
+    with pytest.raises(ValueError, match="invalid key range"):
+        DenseAggregationSlab(5, 4, torch.int64, [], [], "cpu")
+    with pytest.raises(ValueError, match="unsupported slab reduction"):
+        DenseAggregationSlab(0, 4, torch.int64, [(torch.int64, ())], ["mean"], "cpu")
