@@ -197,10 +197,12 @@ int pf_slab_finish(const uint8_t* occupied, int64_t key_min, int64_t capacity, i
  * (the value is then price).  Sums are exact int64 (wrapping on overflow as
  * int64 arithmetic does).  Outputs: sum_out / count_out [n_groups] (zero for
  * groups no row reached; a group is present iff its count > 0) and, in
- * stats_out (device int64[4]): matched probe rows, 0 (reserved), build rows
- * whose group is out of range (their matches are not aggregated), and the
- * number of build rows no table slot took (0 on success).  Waits once, for
- * the bucket counts that plan the rounds; the rest stays queued.
+ * stats_out (device int64[4]): matched probe rows, the device error word (0,
+ * or nonzero when a kernel gave up a bounded wait for its bulk copies; the
+ * outputs are then not valid), build rows whose group is out of range (their
+ * matches are not aggregated), and the number of build rows no table slot
+ * took (0 on success).  Waits once, for the bucket counts that plan the
+ * rounds; the rest stays queued.
  */
 size_t pf_join_aggregate_workspace(int64_t n_build, int64_t n_probe, int B, int64_t n_groups);
 int pf_join_aggregate(const int64_t* build_key, const int32_t* build_group, int64_t n_build,

@@ -8,7 +8,12 @@ from pathlib import Path
 
 import torch
 
-LIB_PATH = Path(__file__).resolve().parent / "libpageflow_b200.so"
+import os
+
+# The in-tree build; PAGEFLOW_B200_LIB names another build of the same
+# sources (e.g. one compiled with different tuning macros).
+LIB_PATH = Path(os.environ.get("PAGEFLOW_B200_LIB",
+                               Path(__file__).resolve().parent / "libpageflow_b200.so"))
 
 PF_OK = 0
 PF_EINVAL = -1

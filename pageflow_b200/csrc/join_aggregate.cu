@@ -31,6 +31,7 @@
 #include <vector>
 
 #include "scan.cuh"
+#include "tma.cuh"
 
 namespace pf {
 namespace {
@@ -40,7 +41,25 @@ constexpr int FITEMS = 8;
 constexpr int FSUB = FT * FITEMS;  // rows of a scatter sub-tile
 constexpr int FB_MAX = 4096;       // fan-out limit
 constexpr int PT2 = 256;           // threads of build / probe
-constexpr int PITEMS2 = 4;         // rows a probe thread keeps in flight
+// Tunables of the round kernels (rows a thread keeps in flight, minimum
+// resident blocks per SM, grid in blocks per SM); compile-time so that ptxas
+// sizes the registers for them.
+#ifndef PF_PITEMS
+#define PF_PITEMS 1
+#endif
+#ifndef PF_PROBE_MINB
+#define PF_PROBE_MINB 8
+#endif
+#ifndef PF_PROBE_GRID
+#define PF_PROBE_GRID 8
+#endif
+#ifndef PF_BUILD_MINB
+#define PF_BUILD_MINB 8
+#endif
+#ifndef PF_BUILD_GRID
+#define PF_BUILD_GRID 8
+#endif
+constexpr int PITEMS2 = PF_PITEMS;   // rows a probe thread keeps in flight
 constexpr long long ROUND_ROWS_DEFAULT = 1536 * 1024;  // build rows a round's table holds
 
 struct Slot {
@@ -48,10 +67,6 @@ struct Slot {
   unsigned long long tagged;  // (tag << 32) | group offset
 };
 
-__device__ __forceinline__ Slot load_slot(const Slot* p) {
-  const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(p);
-  return Slot{v.x, v.y};
-}
 
 // ---- 1. histograms ------------------------------------------------------------
 
@@ -231,6 +246,236 @@ size_t fscatter_smem(int B, bool probe) {
   return s;
 }
 
+// ---- 3'. the scatter fed by bulk asynchronous copies -----------------------------------
+
+// The same scatter with each 2048-row sub-tile's source columns brought into
+// shared memory by bulk copies (the TMA engine) up to TNBUF sub-tiles ahead,
+// so the reads of later sub-tiles overlap the ranking, staging and writes of
+// the current one.  Used when every source column is 16-byte aligned; the
+// bytes of a final partial sub-tile past its last whole 16 come from global
+// loads.  A bulk copy that never lands (bounded waits) sets *err and the
+// CTA stops after waiting, again bounded, for its copies still in flight.
+constexpr int TT = 512;
+// rows of a sub-tile: 2048 for the probe side (24 B a row in), 4096 for the
+// build side (12 B a row in)
+template <bool PROBE>
+struct TSub {
+  static constexpr int rows = PROBE ? 2048 : 4096;
+};
+
+struct TmaCols {
+  const void* src[3];
+  int es[3];
+  int ncols;
+};
+
+template <bool PROBE>
+struct TmaSmem {
+  static constexpr int TSUB = TSub<PROBE>::rows;
+  // offsets (bytes) of each region for B buckets and nbuf buffers
+  size_t bar, in, stage_key, stage_val, sbk, base, cnt, tstart, wsum, flag, total;
+  size_t in_stride;  // bytes of one buffer
+  __host__ __device__ TmaSmem(int B, int nbuf) {
+    const size_t rowb = PROBE ? 24 : 12;
+    size_t o = 0;
+    bar = o;
+    o += 128;
+    in = o;
+    in_stride = (size_t)TSUB * rowb;
+    o += (size_t)nbuf * in_stride;
+    stage_key = o;
+    o += (size_t)TSUB * 8;
+    stage_val = o;
+    o += (size_t)TSUB * (PROBE ? 8 : 4);
+    sbk = o;
+    o += (size_t)TSUB * 2;
+    o = (o + 15) / 16 * 16;
+    base = o;
+    o += (size_t)B * 8;
+    cnt = o;
+    o += (size_t)B * 4;
+    tstart = o;
+    o += (size_t)B * 4;
+    wsum = o;
+    o += 32 * 4;
+    flag = o;
+    o += 16;
+    total = (o + 127) / 128 * 128;
+  }
+};
+
+template <bool PROBE>
+__global__ void __launch_bounds__(TT) k_fscatter_tma(const long long* __restrict__ key,
+                                                     const void* __restrict__ v0,
+                                                     const long long* __restrict__ v1,
+                                                     long long scale, long long n, long long chunk,
+                                                     int logB, int B, int nbuf,
+                                                     const int* __restrict__ hist,
+                                                     const long long* __restrict__ start,
+                                                     long long* __restrict__ okey,
+                                                     void* __restrict__ oval,
+                                                     unsigned long long* err) {
+  using V = typename std::conditional<PROBE, long long, int>::type;
+  constexpr int TSUB = TSub<PROBE>::rows;
+  constexpr int TROWS = TSUB / TT;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const TmaSmem<PROBE> L(B, nbuf);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + L.bar);
+  unsigned long long* skey = reinterpret_cast<unsigned long long*>(smem + L.stage_key);
+  V* sval = reinterpret_cast<V*>(smem + L.stage_val);
+  unsigned short* sbk = reinterpret_cast<unsigned short*>(smem + L.sbk);
+  long long* base = reinterpret_cast<long long*>(smem + L.base);
+  int* cnt = reinterpret_cast<int*>(smem + L.cnt);
+  int* tstart = reinterpret_cast<int*>(smem + L.tstart);
+  int* wsum = reinterpret_cast<int*>(smem + L.wsum);
+
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const long long lo = (long long)blockIdx.x * chunk;
+  const long long hi = min(n, lo + chunk);
+  const int ntiles = lo < hi ? (int)((hi - lo + TSUB - 1) / TSUB) : 0;
+  const int ncols = PROBE ? (v1 ? 3 : 2) : 2;
+  const void* src[3] = {key, v0, v1};
+  const int es[3] = {8, PROBE ? 8 : 4, 8};
+  // column c of buffer b: in + b*in_stride + colofs[c]
+  const size_t colofs[3] = {0, (size_t)TSUB * 8, (size_t)TSUB * (PROBE ? 16 : 12)};
+
+  auto tma_rows = [&](int c, int rows) -> int { return (rows * es[c]) / 16 * 16 / es[c]; };
+  auto issue = [&](int t) {
+    const int b = t % nbuf;
+    const long long sb = lo + (long long)t * TSUB;
+    const int rows = (int)min((long long)TSUB, hi - sb);
+    unsigned bytes = 0;
+    for (int c = 0; c < ncols; ++c) bytes += (unsigned)(tma_rows(c, rows) * es[c]);
+    mbar_arrive_expect_tx(&bar[b], bytes);
+    for (int c = 0; c < ncols; ++c) {
+      const unsigned nb = (unsigned)(tma_rows(c, rows) * es[c]);
+      if (nb)
+        bulk_g2s(smem + L.in + b * L.in_stride + colofs[c],
+                 reinterpret_cast<const char*>(src[c]) + sb * es[c], nb, &bar[b]);
+    }
+  };
+
+  if (tid == 0) {
+    for (int b = 0; b < nbuf; ++b) mbar_init(&bar[b], 1);
+    mbar_init_fence();
+  }
+  const int* hrow = hist + (long long)blockIdx.x * B;
+  for (int b = tid; b < B; b += TT) base[b] = start[b] + hrow[b];
+  __syncthreads();
+  if (tid == 0)
+    for (int t = 0; t < min(nbuf, ntiles); ++t) issue(t);
+
+  const V* g0 = reinterpret_cast<const V*>(v0);
+  V* out0 = reinterpret_cast<V*>(oval);
+  for (int t = 0; t < ntiles; ++t) {
+    const int b_ = t % nbuf;
+    const unsigned parity = (unsigned)((t / nbuf) & 1);
+    const long long sb = lo + (long long)t * TSUB;
+    const int rows = (int)min((long long)TSUB, hi - sb);
+    for (int b = tid; b < B; b += TT) cnt[b] = 0;
+    const bool ok = mbar_wait_bounded(&bar[b_], parity);
+    if (__syncthreads_or(!ok)) {
+      // a copy never landed: report, let the copies in flight finish, stop
+      if (tid == 0) {
+        atomicOr(err, 1ULL);
+        for (int u = t; u < min(ntiles, t + nbuf); ++u)
+          mbar_wait_bounded(&bar[u % nbuf], (unsigned)((u / nbuf) & 1), 1u << 16);
+      }
+      __syncthreads();
+      return;
+    }
+    const unsigned char* ib = smem + L.in + b_ * L.in_stride;
+    const unsigned long long* ik = reinterpret_cast<const unsigned long long*>(ib + colofs[0]);
+    const V* iv = reinterpret_cast<const V*>(ib + colofs[1]);
+    const long long* id = reinterpret_cast<const long long*>(ib + colofs[2]);
+    const int tk = tma_rows(0, rows), tv = tma_rows(1, rows), td = tma_rows(2, rows);
+    unsigned long long kv[TROWS];
+    V vv[TROWS];
+    int bk[TROWS], rk[TROWS];
+#pragma unroll
+    for (int k = 0; k < TROWS; ++k) {
+      const int r = k * TT + tid;
+      bk[k] = -1;
+      if (r < rows) {
+        kv[k] = r < tk ? ik[r] : (unsigned long long)key[sb + r];
+        if (PROBE) {
+          const long long price = r < tv ? (long long)iv[r] : reinterpret_cast<const long long*>(v0)[sb + r];
+          if (v1) {
+            const long long d = r < td ? id[r] : v1[sb + r];
+            vv[k] = (V)(long long)((unsigned long long)price * (unsigned long long)(scale - d));
+          } else {
+            vv[k] = (V)price;
+          }
+        } else {
+          vv[k] = r < tv ? iv[r] : g0[sb + r];
+        }
+        bk[k] = bucket_of_hash(mix64(kv[k]), logB);
+        rk[k] = atomicAdd(&cnt[bk[k]], 1);
+      }
+    }
+    __syncthreads();
+    {
+      const int per = (B + TT - 1) / TT;
+      const int b0 = tid * per;
+      int s = 0;
+      for (int q = 0; q < per; ++q)
+        if (b0 + q < B) s += cnt[b0 + q];
+      int incl = s;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += y;
+      }
+      if (lane == 31) wsum[w] = incl;
+      __syncthreads();
+      int pre = 0;
+      for (int q = 0; q < TT / 32; ++q) pre += q < w ? wsum[q] : 0;
+      int ex = pre + incl - s;
+      for (int q = 0; q < per; ++q) {
+        if (b0 + q < B) {
+          tstart[b0 + q] = ex;
+          ex += cnt[b0 + q];
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < TROWS; ++k) {
+      if (bk[k] >= 0) {
+        const int s = tstart[bk[k]] + rk[k];
+        skey[s] = kv[k];
+        sval[s] = vv[k];
+        sbk[s] = (unsigned short)bk[k];
+      }
+    }
+    __syncthreads();
+    // this buffer is consumed: refill it with the sub-tile nbuf ahead
+    if (tid == 0 && t + nbuf < ntiles) {
+      fence_proxy_async_smem();
+      issue(t + nbuf);
+    }
+    for (int s = tid; s < rows; s += TT) {
+      const int b = sbk[s];
+      const long long pos = base[b] + (s - tstart[b]);
+      okey[pos] = (long long)skey[s];
+      out0[pos] = sval[s];
+    }
+    __syncthreads();
+    for (int b = tid; b < B; b += TT) base[b] += cnt[b];
+  }
+}
+
+template <bool PROBE>
+int tma_nbuf(int B) {
+  return TmaSmem<PROBE>(B, 3).total <= 220 * 1024 ? 3 : 2;
+}
+
+template <bool PROBE>
+size_t tma_smem(int B) {
+  return TmaSmem<PROBE>(B, tma_nbuf<PROBE>(B)).total;
+}
+
+bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
+
 // ---- 4. rounds: build and probe ----------------------------------------------------
 
 struct RoundArgs {
@@ -243,60 +488,73 @@ struct RoundArgs {
   Slot* table;
   const long long* reg_off;  // [B] slot offset of each partition's region
   const long long* reg_cap;  // [B] slots of each partition's region
+  int p0, p1;                // the round's partitions
   long long slice_cap;       // > 0: a slice round, one region of this size at 0
   unsigned tag;
   int logB;
   long long group_min, n_groups;
-  unsigned long long* sum;
-  unsigned long long* count;
+  unsigned long long* slab;   // [2 * n_groups]: (sum, count) of group g at 2g, 2g+1
   unsigned long long* stats;  // [0] matched, [1] reserved, [2] build rows out of group range, [3] overflow
 };
 
-__device__ __forceinline__ void region_of(const RoundArgs& a, uint64_t h, long long* off,
-                                          long long* cap) {
-  if (a.slice_cap > 0) {
-    *off = 0;
-    *cap = a.slice_cap;
-  } else {
-    const int b = bucket_of_hash(h, a.logB);
-    *off = a.reg_off[b];
-    *cap = a.reg_cap[b];
+// The round's regions, {slot offset, slots} per partition p0..p1-1, staged in
+// shared memory by every block (a slice round has one region).
+__device__ __forceinline__ int stage_regions(const RoundArgs& a, uint2* reg) {
+  const int n = a.slice_cap > 0 ? 1 : a.p1 - a.p0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    if (a.slice_cap > 0) reg[i] = make_uint2(0u, (unsigned)a.slice_cap);
+    else reg[i] = make_uint2((unsigned)a.reg_off[a.p0 + i], (unsigned)a.reg_cap[a.p0 + i]);
   }
+  __syncthreads();
+  return n;
+}
+
+__device__ __forceinline__ uint2 region_of(const RoundArgs& a, const uint2* reg, uint64_t h) {
+  return a.slice_cap > 0 ? reg[0] : reg[bucket_of_hash(h, a.logB) - a.p0];
 }
 
 // The first slot of hash h inside a region of `cap` slots: multiply-shift of
 // the 32 bits right below the bucket bits.
-__device__ __forceinline__ long long first_slot(uint64_t h, int logB, long long cap) {
+__device__ __forceinline__ unsigned first_slot(uint64_t h, int logB, unsigned cap) {
   const uint32_t x = (uint32_t)((h << logB) >> 32);
-  return (long long)(((unsigned long long)x * (unsigned long long)cap) >> 32);
+  return (unsigned)(((unsigned long long)x * cap) >> 32);
 }
 
-__global__ void __launch_bounds__(PT2) k_fbuild(RoundArgs a) {
+__device__ __forceinline__ ulonglong2 ld_slot(const Slot* p) {
+  return __ldcg(reinterpret_cast<const ulonglong2*>(p));
+}
+
+// Build: one row a thread at a time.  A slot is free for this round when its
+// tag (the high half of the tagged word) is below the round's tag (tags grow
+// round by round; the table is zeroed once per call): an atomicMax of the tag
+// claims it without a read first, and only the claimant, seeing an older tag
+// come back, writes the whole slot (key, group, tag) with one 16-byte store.
+// A loser's max leaves the tag as it is.  The probe runs in a later launch.
+__global__ void __launch_bounds__(PT2, PF_BUILD_MINB) k_fbuild(RoundArgs a) {
+  extern __shared__ uint2 reg[];
+  stage_regions(a, reg);
   unsigned long long bad_group = 0, overflow = 0;
   for (long long i = a.b_lo + (long long)blockIdx.x * PT2 + threadIdx.x; i < a.b_hi;
        i += (long long)gridDim.x * PT2) {
-    const long long k = a.bkey[i];
+    const unsigned long long key = (unsigned long long)a.bkey[i];
     const long long g = (long long)a.bgrp[i] - a.group_min;
     uint32_t goff = 0xffffffffu;
     if (g >= 0 && g < a.n_groups) goff = (uint32_t)g;
     else ++bad_group;
-    const uint64_t h = mix64((uint64_t)k);
-    long long off, cap;
-    region_of(a, h, &off, &cap);
-    long long s = first_slot(h, a.logB, cap);
-    const unsigned long long mine = ((unsigned long long)a.tag << 32) | goff;
+    const uint64_t h = mix64(key);
+    const uint2 r = region_of(a, reg, h);
+    unsigned pos = first_slot(h, a.logB, r.y);
     bool done = false;
-    for (long long probes = 0; probes < cap; ++probes) {
-      Slot* sl = a.table + off + s;
-      unsigned long long cur = sl->tagged;
-      if ((uint32_t)(cur >> 32) != a.tag) {
-        if (atomicCAS(&sl->tagged, cur, mine) == cur) {
-          sl->key = (unsigned long long)k;
-          done = true;
-          break;
-        }
+    for (unsigned left = r.y; left > 0; --left) {
+      Slot* sl = a.table + r.x + pos;
+      unsigned* tag = reinterpret_cast<unsigned*>(&sl->tagged) + 1;
+      if (atomicMax(tag, a.tag) < a.tag) {
+        *reinterpret_cast<ulonglong2*>(sl) =
+            make_ulonglong2(key, ((unsigned long long)a.tag << 32) | goff);
+        done = true;
+        break;
       }
-      if (++s == cap) s = 0;
+      if (++pos == r.y) pos = 0;
     }
     overflow += !done;
   }
@@ -304,19 +562,27 @@ __global__ void __launch_bounds__(PT2) k_fbuild(RoundArgs a) {
   if (overflow) atomicAdd(&a.stats[3], overflow);
 }
 
-__global__ void __launch_bounds__(PT2) k_fprobe(RoundArgs a) {
+// Probe: PITEMS2 rows a thread at a time (one by default: occupancy, not
+// per-thread batching, hides the L2 latency best here), every row's first slot
+// loaded before any is examined; a match adds the row's value and 1 into its
+// group's (sum, count) pair, both words in one 16-byte cell of the slab.
+__global__ void __launch_bounds__(PT2, PF_PROBE_MINB) k_fprobe(RoundArgs a) {
+  extern __shared__ uint2 reg[];
+  stage_regions(a, reg);
   unsigned long long matched = 0;
   const long long stride = (long long)gridDim.x * PT2 * PITEMS2;
   for (long long i0 = a.p_lo + ((long long)blockIdx.x * PT2 * PITEMS2) + threadIdx.x;
        i0 < a.p_hi; i0 += stride) {
-    long long key[PITEMS2], val[PITEMS2], off[PITEMS2], cap[PITEMS2], s[PITEMS2];
-    Slot sl[PITEMS2];
+    unsigned long long key[PITEMS2];
+    long long val[PITEMS2];
+    unsigned pos[PITEMS2], off[PITEMS2], cap[PITEMS2];
+    ulonglong2 sl[PITEMS2];
 #pragma unroll
     for (int k = 0; k < PITEMS2; ++k) {
       const long long i = i0 + (long long)k * PT2;
       cap[k] = 0;
       if (i < a.p_hi) {
-        key[k] = a.pfk[i];
+        key[k] = (unsigned long long)a.pfk[i];
         val[k] = a.pval[i];
       }
     }
@@ -324,37 +590,50 @@ __global__ void __launch_bounds__(PT2) k_fprobe(RoundArgs a) {
     for (int k = 0; k < PITEMS2; ++k) {
       const long long i = i0 + (long long)k * PT2;
       if (i < a.p_hi) {
-        const uint64_t h = mix64((uint64_t)key[k]);
-        region_of(a, h, &off[k], &cap[k]);
-        if (cap[k] > 0) {
-          s[k] = first_slot(h, a.logB, cap[k]);
-          sl[k] = load_slot(a.table + off[k] + s[k]);
+        const uint64_t h = mix64(key[k]);
+        const uint2 r = region_of(a, reg, h);
+        off[k] = r.x;
+        cap[k] = r.y;
+        if (r.y > 0) {
+          pos[k] = first_slot(h, a.logB, r.y);
+          sl[k] = ld_slot(a.table + off[k] + pos[k]);
         }
       }
     }
 #pragma unroll
     for (int k = 0; k < PITEMS2; ++k) {
-      if (cap[k] <= 0) continue;
-      long long probes = 0;
+      if (cap[k] == 0) continue;
+      unsigned probes = 0;
       while (true) {
-        if ((uint32_t)(sl[k].tagged >> 32) != a.tag) break;  // a free slot: no match
-        if (sl[k].key == (unsigned long long)key[k]) {
-          const uint32_t g = (uint32_t)sl[k].tagged;
+        if ((uint32_t)(sl[k].y >> 32) != a.tag) break;  // a free slot: no match
+        if (sl[k].x == key[k]) {
+          const uint32_t g = (uint32_t)sl[k].y;
           if (g != 0xffffffffu) {
-            atomicAdd(&a.sum[g], (unsigned long long)val[k]);
-            atomicAdd(&a.count[g], 1ULL);
+            atomicAdd(&a.slab[2 * (unsigned long long)g], (unsigned long long)val[k]);
+            atomicAdd(&a.slab[2 * (unsigned long long)g + 1], 1ULL);
           }
           ++matched;
           break;
         }
         if (++probes >= cap[k]) break;
-        if (++s[k] == cap[k]) s[k] = 0;
-        sl[k] = load_slot(a.table + off[k] + s[k]);
+        if (++pos[k] == cap[k]) pos[k] = 0;
+        sl[k] = ld_slot(a.table + off[k] + pos[k]);
       }
     }
   }
   for (int o = 16; o; o >>= 1) matched += __shfl_xor_sync(FULL, matched, o);
   if ((threadIdx.x & 31) == 0 && matched) atomicAdd(&a.stats[0], matched);
+}
+
+// The interleaved slab split into the caller's sum and count arrays.
+__global__ void k_split(const unsigned long long* __restrict__ slab, long long n,
+                        long long* __restrict__ sum, long long* __restrict__ count) {
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < n;
+       g += (long long)gridDim.x * blockDim.x) {
+    const ulonglong2 v = reinterpret_cast<const ulonglong2*>(slab)[g];
+    sum[g] = (long long)v.x;
+    count[g] = (long long)v.y;
+  }
 }
 
 // The regions of the rounds, from the build counts: the same greedy packing
@@ -458,9 +737,10 @@ struct JaLayout {
   Slot* table;
   long long table_slots;
   long long* reg;      // [2B]: reg_off, reg_cap
+  unsigned long long* slab;  // [2 * n_groups]: (sum, count) per group
 };
 
-JaLayout ja_layout(Arena& a, long long nb, long long np, int B) {
+JaLayout ja_layout(Arena& a, long long nb, long long np, int B, long long n_groups) {
   JaLayout l{};
   long long chunk;
   int nb_ch, np_ch;
@@ -478,6 +758,7 @@ JaLayout ja_layout(Arena& a, long long nb, long long np, int B) {
   l.table_slots = 2 * std::max<long long>(1, std::min(nb, round_rows()));
   l.table = a.take<Slot>(l.table_slots);
   l.reg = a.take<long long>(2 * (size_t)B);
+  l.slab = a.take<unsigned long long>(2 * (size_t)std::max<long long>(n_groups, 1));
   return l;
 }
 
@@ -520,10 +801,9 @@ extern "C" int pf_join_aggregate_pick_b(int64_t n_build, int64_t n_probe) {
 
 extern "C" size_t pf_join_aggregate_workspace(int64_t n_build, int64_t n_probe, int B,
                                               int64_t n_groups) {
-  (void)n_groups;
   if (B < 1) B = 1;
   Arena a(nullptr, 0);
-  ja_layout(a, n_build, n_probe, B);
+  ja_layout(a, n_build, n_probe, B, n_groups);
   return a.used + 256;
 }
 
@@ -543,15 +823,18 @@ extern "C" int pf_join_aggregate(const int64_t* build_key, const int32_t* build_
   if (n_build >= (1LL << 40) || n_probe >= (1LL << 40))
     return fail(PF_EINVAL, "join_aggregate: at most 2^40 rows a side");
   Arena ar(workspace, workspace_bytes);
-  JaLayout l = ja_layout(ar, n_build, n_probe, B);
+  JaLayout l = ja_layout(ar, n_build, n_probe, B, n_groups);
   if (!workspace || !ar.fits())
     return fail(PF_ENOSPACE, "join_aggregate: workspace of %zu bytes, %zu needed",
                 workspace_bytes, ar.used);
   const int logB = log2_exact((uint64_t)B);
-  PF_CUDA(cudaMemsetAsync(sum_out, 0, n_groups * sizeof(long long), st));
-  PF_CUDA(cudaMemsetAsync(count_out, 0, n_groups * sizeof(long long), st));
   PF_CUDA(cudaMemsetAsync(stats_out, 0, 4 * sizeof(long long), st));
-  if (n_build == 0 || n_probe == 0) return ok();
+  if (n_build == 0 || n_probe == 0) {
+    PF_CUDA(cudaMemsetAsync(sum_out, 0, n_groups * sizeof(long long), st));
+    PF_CUDA(cudaMemsetAsync(count_out, 0, n_groups * sizeof(long long), st));
+    return ok();
+  }
+  PF_CUDA(cudaMemsetAsync(l.slab, 0, 2 * n_groups * sizeof(unsigned long long), st));
 
   // 1-2: histograms and offsets of both sides
   long long chunk_b, chunk_p;
@@ -594,20 +877,42 @@ extern "C" int pf_join_aggregate(const int64_t* build_key, const int32_t* build_
   if (int rc = record_event(st, &ev)) return rc;
 
   // 3: the scatters, queued while the host waits for the counts
-  const size_t smb = fscatter_smem(B, false), smp = fscatter_smem(B, true);
-  if (int rc = opt_in_smem((const void*)k_fscatter<false>, smb)) return rc;
-  if (int rc = opt_in_smem((const void*)k_fscatter<true>, smp)) return rc;
-  {
-    PF_KERNEL("k_fscatter_build", st);
-    k_fscatter<false><<<nch_b, FT, smb, st>>>((const long long*)build_key, build_group, nullptr, 0,
-                                              n_build, chunk_b, logB, B, l.hist_b, l.start, l.pkey,
-                                              l.pgrp);
-  }
-  {
-    PF_KERNEL("k_fscatter_probe", st);
-    k_fscatter<true><<<nch_p, FT, smp, st>>>((const long long*)probe_fk, probe_price,
-                                             (const long long*)probe_disc, scale, n_probe, chunk_p,
-                                             logB, B, l.hist_p, l.start + B, l.pfk, l.pval);
+  const bool tma = aligned16(build_key) && aligned16(build_group) && aligned16(probe_fk) &&
+                   aligned16(probe_price) && (!probe_disc || aligned16(probe_disc)) &&
+                   getenv("PF_NO_TMA") == nullptr;
+  if (tma) {
+    const size_t smb = tma_smem<false>(B), smp = tma_smem<true>(B);
+    if (int rc = opt_in_smem((const void*)k_fscatter_tma<false>, smb)) return rc;
+    if (int rc = opt_in_smem((const void*)k_fscatter_tma<true>, smp)) return rc;
+    {
+      PF_KERNEL("k_fscatter_build", st);
+      k_fscatter_tma<false><<<nch_b, TT, smb, st>>>(
+          (const long long*)build_key, build_group, nullptr, 0, n_build, chunk_b, logB, B,
+          tma_nbuf<false>(B), l.hist_b, l.start, l.pkey, l.pgrp, (unsigned long long*)stats_out + 1);
+    }
+    {
+      PF_KERNEL("k_fscatter_probe", st);
+      k_fscatter_tma<true><<<nch_p, TT, smp, st>>>(
+          (const long long*)probe_fk, probe_price, (const long long*)probe_disc, scale, n_probe,
+          chunk_p, logB, B, tma_nbuf<true>(B), l.hist_p, l.start + B, l.pfk, l.pval,
+          (unsigned long long*)stats_out + 1);
+    }
+  } else {
+    const size_t smb = fscatter_smem(B, false), smp = fscatter_smem(B, true);
+    if (int rc = opt_in_smem((const void*)k_fscatter<false>, smb)) return rc;
+    if (int rc = opt_in_smem((const void*)k_fscatter<true>, smp)) return rc;
+    {
+      PF_KERNEL("k_fscatter_build", st);
+      k_fscatter<false><<<nch_b, FT, smb, st>>>((const long long*)build_key, build_group, nullptr, 0,
+                                                n_build, chunk_b, logB, B, l.hist_b, l.start, l.pkey,
+                                                l.pgrp);
+    }
+    {
+      PF_KERNEL("k_fscatter_probe", st);
+      k_fscatter<true><<<nch_p, FT, smp, st>>>((const long long*)probe_fk, probe_price,
+                                               (const long long*)probe_disc, scale, n_probe, chunk_p,
+                                               logB, B, l.hist_p, l.start + B, l.pfk, l.pval);
+    }
   }
   PF_LAUNCH("k_fscatter");
   if (int rc = wait_event(ev)) return rc;
@@ -660,8 +965,7 @@ extern "C" int pf_join_aggregate(const int64_t* build_key, const int32_t* build_
   a.logB = logB;
   a.group_min = group_min;
   a.n_groups = n_groups;
-  a.sum = (unsigned long long*)sum_out;
-  a.count = (unsigned long long*)count_out;
+  a.slab = l.slab;
   a.stats = (unsigned long long*)stats_out;
   const int sms = sm_count();
   for (size_t r = 0; r < rounds.size(); ++r) {
@@ -671,26 +975,35 @@ extern "C" int pf_join_aggregate(const int64_t* build_key, const int32_t* build_
     a.p_lo = R.p_lo;
     a.p_hi = R.p_hi;
     a.slice_cap = R.slice_cap;
+    a.p0 = R.p0;
+    a.p1 = R.p1;
     a.tag = (unsigned)(r + 1);
+    const size_t rsm = (size_t)(R.slice_cap > 0 ? 1 : std::max(1, R.p1 - R.p0)) * sizeof(uint2);
     const long long nbr = R.b_hi - R.b_lo, npr = R.p_hi - R.p_lo;
     if (nbr > 0) {
       const unsigned g = (unsigned)std::max<long long>(
-          1, std::min<long long>((nbr + PT2 - 1) / PT2, (long long)sms * 8));
+          1, std::min<long long>((nbr + PT2 - 1) / PT2, (long long)sms * PF_BUILD_GRID));
       {
         PF_KERNEL("k_fbuild", st);
-        k_fbuild<<<g, PT2, 0, st>>>(a);
+        k_fbuild<<<g, PT2, rsm, st>>>(a);
       }
     }
     if (nbr > 0 && npr > 0) {
       const unsigned g = (unsigned)std::max<long long>(
-          1, std::min<long long>((npr + PT2 * PITEMS2 - 1) / (PT2 * PITEMS2), (long long)sms * 8));
+          1, std::min<long long>((npr + PT2 * PITEMS2 - 1) / (PT2 * PITEMS2), (long long)sms * PF_PROBE_GRID));
       {
         PF_KERNEL("k_fprobe", st);
-        k_fprobe<<<g, PT2, 0, st>>>(a);
+        k_fprobe<<<g, PT2, rsm, st>>>(a);
       }
     }
   }
   PF_LAUNCH("k_fbuild/k_fprobe");
+  {
+    PF_KERNEL("k_split", st);
+    k_split<<<(unsigned)std::max<long long>(1, std::min<long long>((n_groups + 255) / 256, sms * 8LL)),
+              256, 0, st>>>(l.slab, n_groups, (long long*)sum_out, (long long*)count_out);
+  }
+  PF_LAUNCH("k_split");
   return ok();
 }
 

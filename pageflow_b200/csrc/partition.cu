@@ -743,7 +743,10 @@ extern "C" int pf_partition_sort(const void* const* cols_in, void* const* cols_o
     if (comp[c] && !has_mask) return fail(PF_EINVAL, "partition_sort: a compacted column needs the mask");
     const int cl = cls_of(row_bytes[c]);
     if (cl < 0) return fail(PF_EINVAL, "partition_sort: more than %d row widths", MAXCLS);
-    if ((n_dom > 0 && !cols_in[c]) || !cols_out[c])
+    // an empty column may come with a null pointer (torch gives one for 0 rows)
+    const long long in_rows = comp[c] ? n_valid : n_dom;
+    const long long out_rows = n_valid + (long long)B * (pf_rows_per_unit(row_bytes[c]) - 1);
+    if ((in_rows > 0 && !cols_in[c]) || (out_rows > 0 && !cols_out[c]))
       return fail(PF_EINVAL, "partition_sort: column %d has a null pointer", c);
     p.c.in[c] = (const unsigned char*)cols_in[c];
     p.c.out[c] = (unsigned char*)cols_out[c];

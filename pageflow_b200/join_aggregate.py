@@ -26,6 +26,7 @@ class JoinAggregateStats:
     matched: int          # probe rows that found their build row
     bad_groups: int       # build rows whose group lay outside the range
     overflow: int         # build rows no table slot took (0 unless broken)
+    device_error: int     # nonzero: a kernel gave up a bounded wait (results invalid)
 
 
 class JoinAggregate:
@@ -97,7 +98,8 @@ class JoinAggregate:
 
     def read_stats(self) -> JoinAggregateStats:
         s = self.stats.tolist()
-        return JoinAggregateStats(matched=s[0], bad_groups=s[2], overflow=s[3])
+        return JoinAggregateStats(matched=s[0], bad_groups=s[2], overflow=s[3],
+                                  device_error=s[1])
 
 
 def join_group_aggregate(build_key, build_group, probe_fk, probe_price, probe_disc=None,

@@ -117,6 +117,7 @@ def test_small_workload_is_the_references_result():
     assert np.array_equal(counts.cpu().numpy(), g["counts"])
     st = plan.read_stats()
     assert st.matched == int(g["matched"][0]) and st.overflow == 0 and st.bad_groups == 0
+    assert st.device_error == 0
 
 
 def test_device_generator_is_the_cpu_generator():
@@ -140,7 +141,7 @@ def test_every_fan_out_matches_the_oracle(B):
     plan = JoinAggregate(w.n_build, w.n_probe, 0, w.n_groups, "cuda", B=B)
     _assert_groups(plan.run(bkey, bgrp, fk, price, disc), want)
     st = plan.read_stats()
-    assert st.matched == want[3] and st.overflow == 0
+    assert st.matched == want[3] and st.overflow == 0 and st.device_error == 0
 
 
 def test_partitions_over_the_table_budget_take_slices(monkeypatch):

@@ -230,7 +230,7 @@ def test_masked_ticks_at_one_to_512_buckets(below, B, monkeypatch):
     cols = _table(n, ["i64", "s25"], seed=98)
     mask = _mask(n, 0.37, seed=99)
     _check(cols, 0, mask, 0, B)
-    _check(cols, 0, mask, 0, B, compact=[False] * 2, count=True)
+    _check(cols, 0, mask, 0, B, compact=[False] * 3, count=True)
 
 
 def test_uint8_mask_and_bool_mask_agree():
