@@ -50,6 +50,9 @@ def parse_args(argv=None):
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain-form", action="store_true",
+                    help="skip timing the reference's own GPU path")
+    ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--cpu-sample", type=float, default=0.01,
                     help="fraction of the workload the CPU baseline joins per sample")
     return ap.parse_args(argv)
@@ -320,6 +323,11 @@ def run_ours(args, w, world, rank, local_rank):
     if not args.no_e2e:
         e2e = run_e2e(args, w, plan, dev, (bkey, bgrp, fk, price, disc), world)
 
+    plain = None
+    if not args.no_plain_form:
+        plain = run_plain_form(args, w, dev, (bkey, bgrp, fk, price, disc), keys, sums, counts,
+                               ms / args.steps)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, threads, desc = cpu_sample_run(w, args.cpu_sample)
@@ -339,9 +347,39 @@ def run_ours(args, w, world, rank, local_rank):
                        "groups_out": n_groups_out, "matched_probe_rows": matched},
             "roofline": roofline, "step_roofline": step_roofline,
             "kernels": kernels,
-            "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
+            "e2e": e2e, "cpu_baseline": cpu, "plain_form": plain, "clocks": clocks,
+            "gpu_launches": launches,
         }
         print(json.dumps(line), flush=True)
+
+
+def run_plain_form(args, w, dev, inputs, keys, sums, counts, our_ms):
+    """The reference's own GPU path on the same inputs (its compiled
+    partition_sort and join_unique_hash kernels, torch between them, composed
+    as its UVM executor does: oracle/plain_form.py), checked equal to ours,
+    then timed with CUDA events over a few steps."""
+    import torch
+    from oracle import plain_form
+    if not plain_form.available():
+        return {"unavailable": "the reference's kernels are not built (oracle/build_ref.sh)"}
+    k, s, c = plain_form.join_aggregate(*inputs, w.scale)
+    same = bool(torch.equal(k, keys) and torch.equal(s, sums) and torch.equal(c, counts))
+    del k, s, c
+    steps = max(1, args.plain_steps)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        plain_form.join_aggregate(*inputs, w.scale)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    torch.cuda.empty_cache()
+    return {"value": (w.n_build + w.n_probe) / (ms / 1e3), "unit": "rows/s", "ms_per_step": ms,
+            "steps": steps, "identical_results": same, "speedup": ms / our_ms,
+            "kind": "the reference's operators/kernels compiled for sm_100a + its torch "
+                    "composition (uvm/join.py, uvm/aggregate.py)"}
 
 
 def run_e2e(args, w, plan, dev, dev_inputs, world):

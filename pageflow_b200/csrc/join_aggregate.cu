@@ -14,11 +14,13 @@
 //                   side carries (fk, value) with value = price * (scale -
 //                   disc) computed on the way, so the price and discount
 //                   columns are read once and never written
-//   4. per round    k_fbuild: the round's build rows into an open-addressing
-//                   table in L2 (16-byte slots {key, group | round tag});
-//                   k_fprobe: each probe row of the round's partitions looks
-//                   its key up and adds its value and 1 into the dense group
-//                   slab (sum, count) with fire-and-forget atomics
+//   4. k_fround     per round, the round's build rows go into an
+//                   open-addressing table in L2 (16-byte slots {key, group |
+//                   round tag}); each probe row of the round's partitions
+//                   looks its key up and adds its value and 1 into the dense
+//                   group slab (sum, count) with fire-and-forget atomics.  One
+//                   launch probes round r while it builds round r + 1 into
+//                   the other half of a double-buffered table
 //
 // A row's bucket is the top log2(B) bits of mix64(key), as in the reference's
 // partition kernel.  A round is a run of whole partitions whose build rows fit
@@ -41,26 +43,20 @@ constexpr int FITEMS = 8;
 constexpr int FSUB = FT * FITEMS;  // rows of a scatter sub-tile
 constexpr int FB_MAX = 4096;       // fan-out limit
 constexpr int PT2 = 256;           // threads of build / probe
-// Tunables of the round kernels (rows a thread keeps in flight, minimum
-// resident blocks per SM, grid in blocks per SM); compile-time so that ptxas
-// sizes the registers for them.
-#ifndef PF_PITEMS
-#define PF_PITEMS 1
-#endif
+// Tunables of the round kernel (minimum resident blocks per SM, which caps
+// its registers, and the grid in blocks per SM).  One row a thread at a time
+// with full occupancy measured fastest on B200: per-thread batches of rows
+// lost more to divergent probe chains than they gained in parallelism.
 #ifndef PF_PROBE_MINB
 #define PF_PROBE_MINB 8
 #endif
 #ifndef PF_PROBE_GRID
 #define PF_PROBE_GRID 8
 #endif
-#ifndef PF_BUILD_MINB
-#define PF_BUILD_MINB 8
-#endif
-#ifndef PF_BUILD_GRID
-#define PF_BUILD_GRID 8
-#endif
-constexpr int PITEMS2 = PF_PITEMS;   // rows a probe thread keeps in flight
-constexpr long long ROUND_ROWS_DEFAULT = 1536 * 1024;  // build rows a round's table holds
+
+// Build rows a round's table half holds (1.2M: two whole partitions of the
+// 150M-row build at B = 256, whose scatter is far cheaper than B = 512's).
+constexpr long long ROUND_ROWS_DEFAULT = 1200 * 1024;
 
 struct Slot {
   unsigned long long key;
@@ -255,12 +251,20 @@ size_t fscatter_smem(int B, bool probe) {
 // bytes of a final partial sub-tile past its last whole 16 come from global
 // loads.  A bulk copy that never lands (bounded waits) sets *err and the
 // CTA stops after waiting, again bounded, for its copies still in flight.
-constexpr int TT = 512;
-// rows of a sub-tile: 2048 for the probe side (24 B a row in), 4096 for the
-// build side (12 B a row in)
+#ifndef PF_TT
+#define PF_TT 512
+#endif
+#ifndef PF_TSUB_P
+#define PF_TSUB_P 2048
+#endif
+#ifndef PF_TSUB_B
+#define PF_TSUB_B 4096
+#endif
+constexpr int TT = PF_TT;
+// rows of a sub-tile: the probe side carries 24 B a row in, the build side 12
 template <bool PROBE>
 struct TSub {
-  static constexpr int rows = PROBE ? 2048 : 4096;
+  static constexpr int rows = PROBE ? PF_TSUB_P : PF_TSUB_B;
 };
 
 struct TmaCols {
@@ -497,18 +501,6 @@ struct RoundArgs {
   unsigned long long* stats;  // [0] matched, [1] reserved, [2] build rows out of group range, [3] overflow
 };
 
-// The round's regions, {slot offset, slots} per partition p0..p1-1, staged in
-// shared memory by every block (a slice round has one region).
-__device__ __forceinline__ int stage_regions(const RoundArgs& a, uint2* reg) {
-  const int n = a.slice_cap > 0 ? 1 : a.p1 - a.p0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    if (a.slice_cap > 0) reg[i] = make_uint2(0u, (unsigned)a.slice_cap);
-    else reg[i] = make_uint2((unsigned)a.reg_off[a.p0 + i], (unsigned)a.reg_cap[a.p0 + i]);
-  }
-  __syncthreads();
-  return n;
-}
-
 __device__ __forceinline__ uint2 region_of(const RoundArgs& a, const uint2* reg, uint64_t h) {
   return a.slice_cap > 0 ? reg[0] : reg[bucket_of_hash(h, a.logB) - a.p0];
 }
@@ -524,105 +516,191 @@ __device__ __forceinline__ ulonglong2 ld_slot(const Slot* p) {
   return __ldcg(reinterpret_cast<const ulonglong2*>(p));
 }
 
-// Build: one row a thread at a time.  A slot is free for this round when its
-// tag (the high half of the tagged word) is below the round's tag (tags grow
-// round by round; the table is zeroed once per call): an atomicMax of the tag
-// claims it without a read first, and only the claimant, seeing an older tag
-// come back, writes the whole slot (key, group, tag) with one 16-byte store.
-// A loser's max leaves the tag as it is.  The probe runs in a later launch.
-__global__ void __launch_bounds__(PT2, PF_BUILD_MINB) k_fbuild(RoundArgs a) {
-  extern __shared__ uint2 reg[];
-  stage_regions(a, reg);
-  unsigned long long bad_group = 0, overflow = 0;
-  for (long long i = a.b_lo + (long long)blockIdx.x * PT2 + threadIdx.x; i < a.b_hi;
-       i += (long long)gridDim.x * PT2) {
-    const unsigned long long key = (unsigned long long)a.bkey[i];
-    const long long g = (long long)a.bgrp[i] - a.group_min;
-    uint32_t goff = 0xffffffffu;
-    if (g >= 0 && g < a.n_groups) goff = (uint32_t)g;
-    else ++bad_group;
-    const uint64_t h = mix64(key);
-    const uint2 r = region_of(a, reg, h);
-    unsigned pos = first_slot(h, a.logB, r.y);
-    bool done = false;
-    for (unsigned left = r.y; left > 0; --left) {
-      Slot* sl = a.table + r.x + pos;
-      unsigned* tag = reinterpret_cast<unsigned*>(&sl->tagged) + 1;
-      if (atomicMax(tag, a.tag) < a.tag) {
-        *reinterpret_cast<ulonglong2*>(sl) =
-            make_ulonglong2(key, ((unsigned long long)a.tag << 32) | goff);
-        done = true;
-        break;
-      }
-      if (++pos == r.y) pos = 0;
+// Build one row.  A slot is free for this round when its tag (the high half
+// of the tagged word) is below the round's tag (tags grow round by round; the
+// table is zeroed once per call): an atomicMax of the tag claims it without a
+// read first, and only the claimant, seeing an older tag come back, writes the
+// whole slot (key, group, tag) with one 16-byte store.  A loser's max leaves
+// the tag as it is.  The round's probe runs in a later launch.
+__device__ __forceinline__ void build_row(const RoundArgs& a, const uint2* reg, long long i,
+                                          unsigned long long& bad_group,
+                                          unsigned long long& overflow) {
+  const unsigned long long key = (unsigned long long)a.bkey[i];
+  const long long g = (long long)a.bgrp[i] - a.group_min;
+  uint32_t goff = 0xffffffffu;
+  if (g >= 0 && g < a.n_groups) goff = (uint32_t)g;
+  else ++bad_group;
+  const uint64_t h = mix64(key);
+  const uint2 r = region_of(a, reg, h);
+  unsigned pos = first_slot(h, a.logB, r.y);
+  for (unsigned left = r.y; left > 0; --left) {
+    Slot* sl = a.table + r.x + pos;
+    unsigned* tag = reinterpret_cast<unsigned*>(&sl->tagged) + 1;
+    if (atomicMax(tag, a.tag) < a.tag) {
+      *reinterpret_cast<ulonglong2*>(sl) =
+          make_ulonglong2(key, ((unsigned long long)a.tag << 32) | goff);
+      return;
     }
-    overflow += !done;
+    if (++pos == r.y) pos = 0;
   }
-  if (bad_group) atomicAdd(&a.stats[2], bad_group);
-  if (overflow) atomicAdd(&a.stats[3], overflow);
+  ++overflow;
 }
 
-// Probe: PITEMS2 rows a thread at a time (one by default: occupancy, not
-// per-thread batching, hides the L2 latency best here), every row's first slot
-// loaded before any is examined; a match adds the row's value and 1 into its
+// Probe one row: its slots from the first (multiply-shift) one on until a
+// free slot (no match) or its key; a match adds the row's value and 1 into its
 // group's (sum, count) pair, both words in one 16-byte cell of the slab.
-__global__ void __launch_bounds__(PT2, PF_PROBE_MINB) k_fprobe(RoundArgs a) {
-  extern __shared__ uint2 reg[];
-  stage_regions(a, reg);
-  unsigned long long matched = 0;
-  const long long stride = (long long)gridDim.x * PT2 * PITEMS2;
-  for (long long i0 = a.p_lo + ((long long)blockIdx.x * PT2 * PITEMS2) + threadIdx.x;
-       i0 < a.p_hi; i0 += stride) {
-    unsigned long long key[PITEMS2];
-    long long val[PITEMS2];
-    unsigned pos[PITEMS2], off[PITEMS2], cap[PITEMS2];
-    ulonglong2 sl[PITEMS2];
+__device__ __forceinline__ void probe_row(const RoundArgs& a, const uint2* reg, long long i,
+                                          unsigned long long& matched) {
+  const unsigned long long key = (unsigned long long)a.pfk[i];
+  const uint64_t h = mix64(key);
+  const uint2 r = region_of(a, reg, h);
+  if (r.y == 0) return;
+  unsigned pos = first_slot(h, a.logB, r.y);
+  ulonglong2 sl = ld_slot(a.table + r.x + pos);
+  const long long val = a.pval[i];
+  for (unsigned probes = 1;; ++probes) {
+    if ((uint32_t)(sl.y >> 32) != a.tag) return;  // a free slot: no match
+    if (sl.x == key) {
+      const uint32_t g = (uint32_t)sl.y;
+      if (g != 0xffffffffu) {
+        atomicAdd(&a.slab[2 * (unsigned long long)g], (unsigned long long)val);
+        atomicAdd(&a.slab[2 * (unsigned long long)g + 1], 1ULL);
+      }
+      ++matched;
+      return;
+    }
+    if (probes >= r.y) return;
+    if (++pos == r.y) pos = 0;
+    sl = ld_slot(a.table + r.x + pos);
+  }
+}
+
+// cp.async (16 or 8 bytes, global -> shared, not through registers).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+}
+
+// Probe PR rows a thread (rows lo + k*PT2 + tid): every row's first slot
+// and value are gathered into shared memory by cp.async before any is
+// examined, so a thread keeps PR lookups in flight without holding them in
+// registers; a collision continues with plain loads.
+#ifndef PF_PR
+#define PF_PR 2
+#endif
+constexpr int PR = PF_PR;
+constexpr int PUROWS = PT2 * PR;
+
+struct ProbeStage {
+  ulonglong2 slot[PR][PT2];
+  long long val[PR][PT2];
+};
+
+__device__ __forceinline__ void probe_unit(const RoundArgs& a, const uint2* reg, long long lo,
+                                           long long hi, ProbeStage& st,
+                                           unsigned long long& matched) {
+  const int tid = threadIdx.x;
+  unsigned long long key[PR];
+  unsigned pos[PR];
+  uint2 rg[PR];
 #pragma unroll
-    for (int k = 0; k < PITEMS2; ++k) {
-      const long long i = i0 + (long long)k * PT2;
-      cap[k] = 0;
-      if (i < a.p_hi) {
-        key[k] = (unsigned long long)a.pfk[i];
-        val[k] = a.pval[i];
+  for (int k = 0; k < PR; ++k) {
+    const long long i = lo + k * PT2 + tid;
+    rg[k] = make_uint2(0u, 0u);
+    if (i < hi) {
+      key[k] = (unsigned long long)a.pfk[i];
+      const uint64_t h = mix64(key[k]);
+      rg[k] = region_of(a, reg, h);
+      if (rg[k].y) {
+        pos[k] = first_slot(h, a.logB, rg[k].y);
+        cp_async16(&st.slot[k][tid], a.table + rg[k].x + pos[k]);
+        cp_async8(&st.val[k][tid], a.pval + i);
       }
     }
+  }
+  cp_async_wait_all();
 #pragma unroll
-    for (int k = 0; k < PITEMS2; ++k) {
-      const long long i = i0 + (long long)k * PT2;
-      if (i < a.p_hi) {
-        const uint64_t h = mix64(key[k]);
-        const uint2 r = region_of(a, reg, h);
-        off[k] = r.x;
-        cap[k] = r.y;
-        if (r.y > 0) {
-          pos[k] = first_slot(h, a.logB, r.y);
-          sl[k] = ld_slot(a.table + off[k] + pos[k]);
+  for (int k = 0; k < PR; ++k) {
+    if (rg[k].y == 0) continue;
+    ulonglong2 sl = st.slot[k][tid];
+    for (unsigned probes = 1;; ++probes) {
+      if ((uint32_t)(sl.y >> 32) != a.tag) break;  // a free slot: no match
+      if (sl.x == key[k]) {
+        const uint32_t g = (uint32_t)sl.y;
+        if (g != 0xffffffffu) {
+          atomicAdd(&a.slab[2 * (unsigned long long)g], (unsigned long long)st.val[k][tid]);
+          atomicAdd(&a.slab[2 * (unsigned long long)g + 1], 1ULL);
         }
+        ++matched;
+        break;
       }
+      if (probes >= rg[k].y) break;
+      if (++pos[k] == rg[k].y) pos[k] = 0;
+      sl = ld_slot(a.table + rg[k].x + pos[k]);
     }
-#pragma unroll
-    for (int k = 0; k < PITEMS2; ++k) {
-      if (cap[k] == 0) continue;
-      unsigned probes = 0;
-      while (true) {
-        if ((uint32_t)(sl[k].y >> 32) != a.tag) break;  // a free slot: no match
-        if (sl[k].x == key[k]) {
-          const uint32_t g = (uint32_t)sl[k].y;
-          if (g != 0xffffffffu) {
-            atomicAdd(&a.slab[2 * (unsigned long long)g], (unsigned long long)val[k]);
-            atomicAdd(&a.slab[2 * (unsigned long long)g + 1], 1ULL);
-          }
-          ++matched;
-          break;
-        }
-        if (++probes >= cap[k]) break;
-        if (++pos[k] == cap[k]) pos[k] = 0;
-        sl[k] = ld_slot(a.table + off[k] + pos[k]);
-      }
+  }
+}
+
+// One launch of the round pipeline: probe round r (pa, its table half) while
+// building round r + 1 (ba, the other half).  Blocks take work units of
+// UROWS rows from a per-launch counter; build units are spread evenly among
+// the probe units, so the build's claim round trips overlap the probe's L2
+// traffic across the whole launch.  Kernel boundaries give the ordering: a
+// round's table is complete before its probe launch, and a half is probed to
+// the end before the launch that rebuilds it.
+constexpr int UROWS = 1024;
+
+__global__ void __launch_bounds__(PT2, PF_PROBE_MINB) k_fround(RoundArgs pa, RoundArgs ba,
+                                                             unsigned* counter, int units_p,
+                                                             int units_b) {
+  extern __shared__ __align__(16) unsigned char fr_smem[];
+  __shared__ int unit;
+  ProbeStage& stage = *reinterpret_cast<ProbeStage*>(fr_smem);
+  uint2* regs = reinterpret_cast<uint2*>(fr_smem + sizeof(ProbeStage));
+  const int np = pa.p_hi > pa.p_lo ? (pa.slice_cap > 0 ? 1 : pa.p1 - pa.p0) : 0;
+  const int nbr = ba.b_hi > ba.b_lo ? (ba.slice_cap > 0 ? 1 : ba.p1 - ba.p0) : 0;
+  uint2* regp = regs;
+  uint2* regb = regs + np;
+  for (int i = threadIdx.x; i < np; i += blockDim.x)
+    regp[i] = pa.slice_cap > 0 ? make_uint2(0u, (unsigned)pa.slice_cap)
+                               : make_uint2((unsigned)pa.reg_off[pa.p0 + i],
+                                            (unsigned)pa.reg_cap[pa.p0 + i]);
+  for (int i = threadIdx.x; i < nbr; i += blockDim.x)
+    regb[i] = ba.slice_cap > 0 ? make_uint2(0u, (unsigned)ba.slice_cap)
+                               : make_uint2((unsigned)ba.reg_off[ba.p0 + i],
+                                            (unsigned)ba.reg_cap[ba.p0 + i]);
+  unsigned long long matched = 0, bad_group = 0, overflow = 0;
+  const long long U = (long long)units_p + units_b;
+  while (true) {
+    __syncthreads();
+    if (threadIdx.x == 0) unit = (int)atomicAdd(counter, 1u);
+    __syncthreads();
+    const long long u = unit;
+    if (u >= U) break;
+    const long long nb_upto = (u + 1) * units_b / U;  // build units among [0, u]
+    const bool build = nb_upto > u * units_b / U;
+    if (build) {
+      const long long lo = ba.b_lo + (nb_upto - 1) * UROWS;
+      const long long hi = min(ba.b_hi, lo + UROWS);
+      for (long long i = lo + threadIdx.x; i < hi; i += PT2) build_row(ba, regb, i, bad_group, overflow);
+    } else {
+      const long long lo = pa.p_lo + (u - nb_upto) * UROWS;
+      const long long hi = min(pa.p_hi, lo + UROWS);
+      for (long long l0 = lo; l0 < hi; l0 += PUROWS)
+        probe_unit(pa, regp, l0, min(hi, l0 + PUROWS), stage, matched);
     }
   }
   for (int o = 16; o; o >>= 1) matched += __shfl_xor_sync(FULL, matched, o);
-  if ((threadIdx.x & 31) == 0 && matched) atomicAdd(&a.stats[0], matched);
+  if ((threadIdx.x & 31) == 0 && matched) atomicAdd(&pa.stats[0], matched);
+  if (bad_group) atomicAdd(&ba.stats[2], bad_group);
+  if (overflow) atomicAdd(&ba.stats[3], overflow);
 }
 
 // The interleaved slab split into the caller's sum and count arrays.
@@ -716,9 +794,13 @@ long long round_rows() {
   return v;
 }
 
+#ifndef PF_CHUNKS_PER_SM
+#define PF_CHUNKS_PER_SM 2
+#endif
+
 void chunking(long long n, long long* chunk, int* nchunks) {
   const long long subs = std::max<long long>(1, (n + FSUB - 1) / FSUB);
-  const long long want = std::max<long long>(1, (long long)sm_count() * 2);
+  const long long want = std::max<long long>(1, (long long)sm_count() * PF_CHUNKS_PER_SM);
   const long long per = (subs + want - 1) / want;
   *chunk = per * FSUB;
   *nchunks = (int)std::max<long long>(1, (n + *chunk - 1) / *chunk);
@@ -738,6 +820,8 @@ struct JaLayout {
   long long table_slots;
   long long* reg;      // [2B]: reg_off, reg_cap
   unsigned long long* slab;  // [2 * n_groups]: (sum, count) per group
+  long long max_launches;
+  unsigned* counters;        // [max_launches] work counters of the round launches
 };
 
 JaLayout ja_layout(Arena& a, long long nb, long long np, int B, long long n_groups) {
@@ -755,10 +839,15 @@ JaLayout ja_layout(Arena& a, long long nb, long long np, int B, long long n_grou
   l.pgrp = a.take<int>(std::max<long long>(nb, 1));
   l.pfk = a.take<long long>(std::max<long long>(np, 1));
   l.pval = a.take<long long>(std::max<long long>(np, 1));
+  // two halves, one built while the other is probed
   l.table_slots = 2 * std::max<long long>(1, std::min(nb, round_rows()));
-  l.table = a.take<Slot>(l.table_slots);
+  l.table = a.take<Slot>(2 * l.table_slots);
   l.reg = a.take<long long>(2 * (size_t)B);
   l.slab = a.take<unsigned long long>(2 * (size_t)std::max<long long>(n_groups, 1));
+  // one work counter per launch: at most B whole-partition rounds plus the
+  // slices of partitions over the budget, plus one
+  l.max_launches = B + nb / std::max<long long>(1, l.table_slots / 2) + 2;
+  l.counters = a.take<unsigned>(l.max_launches);
   return l;
 }
 
@@ -952,14 +1041,17 @@ extern "C" int pf_join_aggregate(const int64_t* build_key, const int32_t* build_
     k_plan<<<1, 32, 0, st>>>(l.cnt, B, cap_rows, l.reg);
   }
   PF_LAUNCH("k_plan");
-  PF_CUDA(cudaMemsetAsync(l.table, 0, l.table_slots * sizeof(Slot), st));
+  PF_CUDA(cudaMemsetAsync(l.table, 0, 2 * l.table_slots * sizeof(Slot), st));
+  if ((long long)rounds.size() + 1 > l.max_launches)
+    return fail(PF_EINVAL, "join_aggregate: %zu rounds exceed the planned %lld", rounds.size(),
+                l.max_launches - 1);
+  PF_CUDA(cudaMemsetAsync(l.counters, 0, (rounds.size() + 1) * sizeof(unsigned), st));
 
   RoundArgs a{};
   a.bkey = l.pkey;
   a.bgrp = l.pgrp;
   a.pfk = l.pfk;
   a.pval = l.pval;
-  a.table = l.table;
   a.reg_off = l.reg;
   a.reg_cap = l.reg + B;
   a.logB = logB;
@@ -967,37 +1059,49 @@ extern "C" int pf_join_aggregate(const int64_t* build_key, const int32_t* build_
   a.n_groups = n_groups;
   a.slab = l.slab;
   a.stats = (unsigned long long*)stats_out;
-  const int sms = sm_count();
-  for (size_t r = 0; r < rounds.size(); ++r) {
-    const Round& R = rounds[r];
-    a.b_lo = R.b_lo;
-    a.b_hi = R.b_hi;
-    a.p_lo = R.p_lo;
-    a.p_hi = R.p_hi;
-    a.slice_cap = R.slice_cap;
-    a.p0 = R.p0;
-    a.p1 = R.p1;
-    a.tag = (unsigned)(r + 1);
-    const size_t rsm = (size_t)(R.slice_cap > 0 ? 1 : std::max(1, R.p1 - R.p0)) * sizeof(uint2);
-    const long long nbr = R.b_hi - R.b_lo, npr = R.p_hi - R.p_lo;
-    if (nbr > 0) {
-      const unsigned g = (unsigned)std::max<long long>(
-          1, std::min<long long>((nbr + PT2 - 1) / PT2, (long long)sms * PF_BUILD_GRID));
-      {
-        PF_KERNEL("k_fbuild", st);
-        k_fbuild<<<g, PT2, rsm, st>>>(a);
-      }
+  auto round_args = [&](long long r) {
+    RoundArgs x = a;
+    if (r < 0 || r >= (long long)rounds.size()) {
+      x.b_lo = x.b_hi = x.p_lo = x.p_hi = 0;
+      x.p0 = x.p1 = 0;
+      x.slice_cap = 0;
+      x.table = l.table;
+      x.tag = 0;
+      return x;
     }
-    if (nbr > 0 && npr > 0) {
-      const unsigned g = (unsigned)std::max<long long>(
-          1, std::min<long long>((npr + PT2 * PITEMS2 - 1) / (PT2 * PITEMS2), (long long)sms * PF_PROBE_GRID));
-      {
-        PF_KERNEL("k_fprobe", st);
-        k_fprobe<<<g, PT2, rsm, st>>>(a);
-      }
+    const Round& R = rounds[r];
+    x.b_lo = R.b_lo;
+    x.b_hi = R.b_hi;
+    x.p_lo = R.p_lo;
+    x.p_hi = R.p_hi;
+    x.slice_cap = R.slice_cap;
+    x.p0 = R.p0;
+    x.p1 = R.p1;
+    x.tag = (unsigned)(r + 1);
+    x.table = l.table + (r & 1) * l.table_slots;
+    return x;
+  };
+  const int sms = sm_count();
+  // launch k: probe round k - 1 and build round k
+  for (long long k = 0; k <= (long long)rounds.size(); ++k) {
+    RoundArgs pa = round_args(k - 1), ba = round_args(k);
+    if (pa.b_hi == pa.b_lo) pa.p_hi = pa.p_lo;  // no build rows: nothing to match
+    const long long np_rows = pa.p_hi - pa.p_lo, nb_rows = ba.b_hi - ba.b_lo;
+    const int units_p = (int)((np_rows + UROWS - 1) / UROWS);
+    const int units_b = (int)((nb_rows + UROWS - 1) / UROWS);
+    if (units_p + units_b == 0) continue;
+    const int nregp = np_rows > 0 ? (pa.slice_cap > 0 ? 1 : pa.p1 - pa.p0) : 0;
+    const int nregb = nb_rows > 0 ? (ba.slice_cap > 0 ? 1 : ba.p1 - ba.p0) : 0;
+    const size_t rsm = sizeof(ProbeStage) + (size_t)std::max(1, nregp + nregb) * sizeof(uint2);
+    if (int rc = opt_in_smem((const void*)k_fround, rsm)) return rc;
+    const unsigned g = (unsigned)std::max<long long>(
+        1, std::min<long long>(units_p + units_b, (long long)sms * PF_PROBE_GRID));
+    {
+      PF_KERNEL("k_fround", st);
+      k_fround<<<g, PT2, rsm, st>>>(pa, ba, l.counters + k, units_p, units_b);
     }
   }
-  PF_LAUNCH("k_fbuild/k_fprobe");
+  PF_LAUNCH("k_fround");
   {
     PF_KERNEL("k_split", st);
     k_split<<<(unsigned)std::max<long long>(1, std::min<long long>((n_groups + 255) / 256, sms * 8LL)),

@@ -145,7 +145,7 @@ def test_every_fan_out_matches_the_oracle(B):
 
 
 def test_partitions_over_the_table_budget_take_slices(monkeypatch):
-    """B = 1 over 3M build rows: one partition over the 1.5M-row table
+    """B = 1 and 2 over 3M build rows: partitions over the 768K-row table
     budget, joined in slices, each probe row meeting every slice."""
     w = datagen.scaled(datagen.SCALE, 1 / 50)   # 3M x 12M
     bkey, bgrp = datagen.gen_build(w, "cuda")
