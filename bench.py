@@ -53,6 +53,10 @@ def parse_args(argv=None):
     ap.add_argument("--no-plain-form", action="store_true",
                     help="skip timing the reference's own GPU path")
     ap.add_argument("--plain-steps", type=int, default=2)
+    ap.add_argument("--batch-gb", type=float, default=60.0,
+                    help="batch workload: device bytes of one wave")
+    ap.add_argument("--plain-instances", type=int, default=0,
+                    help="batch workload: instances the reference path runs (0: the whole wave)")
     ap.add_argument("--cpu-sample", type=float, default=0.01,
                     help="fraction of the workload the CPU baseline joins per sample")
     return ap.parse_args(argv)
@@ -424,11 +428,107 @@ def run_e2e(args, w, plan, dev, dev_inputs, world):
             "h2d_gbs": h2d / (ms / args.e2e_steps / 1e3) / 1e9}
 
 
+def run_batch(args, world, rank, local_rank):
+    """The batching workload (4,096 instances, seed 3): one wave of whole
+    instances that fits the device (inputs generated on it, untimed), run
+    as one persistent launch replayed from a CUDA graph; beside it the same
+    wave as per-instance launches of the fused path, and the reference's own
+    GPU path per instance on the wave's first instances."""
+    import torch
+    from pageflow_b200 import datagen
+    from pageflow_b200.batch import BatchJoinAggregate, Instance
+    from pageflow_b200.join_aggregate import JoinAggregate
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    specs = datagen.batch_workload(4096, seed=3)
+    budget = args.batch_gb * 1e9
+    wave, used = [], 0.0
+    start = (rank * 997) % len(specs)          # replicas take different waves
+    for j in range(len(specs)):
+        sp = specs[(start + j) % len(specs)]
+        need = sp.n_build * (12 + 32) + sp.n_probe * 16 + sp.n_groups * 16
+        if used + need > budget:
+            continue
+        wave.append(sp)
+        used += need
+    insts = []
+    for sp in wave:
+        key, grp, fk, val = datagen.gen_batch_instance(sp, dev)
+        insts.append(Instance(key, grp, fk, val, 0, sp.n_groups))
+    rows = sum(sp.n_build + sp.n_probe for sp in wave)
+    b = BatchJoinAggregate(insts, dev)
+    g = b.graph()
+    for _ in range(args.warmup):
+        g.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        g.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    st = b.read_stats()
+    # the same instances, one fused-path launch sequence each
+    plans = [JoinAggregate(x.build_key.numel(), x.probe_fk.numel(), 0, x.n_groups, dev,
+                           scale=0) for x in insts]
+    def per_instance():
+        for p, x in zip(plans, insts):
+            p.aggregate(x.build_key, x.build_group, x.probe_fk, x.probe_value, None)
+    per_instance()
+    torch.cuda.synchronize()
+    same = all(torch.equal(p.sum, b.result(i)[0]) and torch.equal(p.count, b.result(i)[1])
+               for i, p in enumerate(plans[:64]))
+    e0.record()
+    per_instance()
+    e1.record()
+    torch.cuda.synchronize()
+    ms_pi = e0.elapsed_time(e1)
+    plain = None
+    from oracle import plain_form
+    if plain_form.available():
+        k = min(len(insts), args.plain_instances or len(insts))
+        sub_rows = sum(insts[i].build_key.numel() + insts[i].probe_fk.numel() for i in range(k))
+        def plain_run():
+            for x in insts[:k]:
+                plain_form.join_aggregate(x.build_key, x.build_group, x.probe_fk,
+                                          x.probe_value, torch.zeros_like(x.probe_value), 1)
+        plain_run()
+        torch.cuda.synchronize()
+        e0.record()
+        plain_run()
+        e1.record()
+        torch.cuda.synchronize()
+        pms = e0.elapsed_time(e1)
+        plain = {"value": sub_rows / (pms / 1e3), "unit": "rows/s", "instances": k,
+                 "ms": pms}
+    if rank == 0:
+        line = {
+            "metric": "join+agg rows/s (batched)", "value": world * rows / (ms / 1e3),
+            "unit": "rows/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded, on device)",
+            "config": {"workload": "batch: 4096 instances (seed 3), one wave",
+                       "wave_instances": len(wave), "wave_rows": rows,
+                       "wave_input_gb": used / 1e9,
+                       "skews": sorted({sp.skew for sp in wave})},
+            "stats": st,
+            "per_instance_launches": {"value": rows / (ms_pi / 1e3), "ms": ms_pi,
+                                      "identical_results": same},
+            "plain_form_per_instance": plain,
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main(argv=None) -> int:
     args = parse_args(argv)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == "batch":
+        run_batch(args, world, rank, local_rank)
+        return 0
     w = workload(args.workload)
     if args.impl == "reference":
         run_reference(args, w, world, rank)

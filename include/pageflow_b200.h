@@ -224,6 +224,43 @@ int pf_groups_finish(const int64_t* sum, const int64_t* count, int64_t group_min
                      int64_t n_groups, int64_t* keys_out, int64_t* sums_out, int64_t* counts_out,
                      int64_t* host_out, void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- batched join -> group-by (many uneven instances, one launch) --------- */
+/*
+ * One instance: SELECT group, SUM(value), COUNT(*) FROM build JOIN probe ON
+ * build.key = probe.fk GROUP BY build.group, a unique build key, groups in
+ * [group_min, group_min + n_groups).  Device pointers; 0 rows allowed.
+ */
+typedef struct {
+  const int64_t* build_key;
+  const int32_t* build_group;
+  int64_t n_build;
+  const int64_t* probe_fk;
+  const int64_t* probe_value;
+  int64_t n_probe;
+  int64_t group_min;
+  int64_t n_groups;
+} pf_batch_instance;
+/*
+ * The batch engine: pf_batch_prepare uploads the instances' descriptors into
+ * the workspace and lays out a hash table per instance (twice its build rows
+ * in 16-byte slots) and a dense (sum, count) slab per instance; it waits
+ * once.  pf_batch_run then queues only device work (a reset of the slabs and
+ * the work counters, then one persistent launch in which blocks take build
+ * and probe work items from a device queue, a probe item waiting, bounded,
+ * for its instance's build items), so it can be captured in a CUDA graph and
+ * replayed; each run bumps a device epoch that tags the table slots, so the
+ * tables are never cleared.  pf_batch_slab gives instance i's slab: int64
+ * pairs (sum, count) per group, interleaved.  stats (device int64[4]):
+ * matched probe rows, device error word (a bounded wait gave up), build rows
+ * out of group range, table overflows.  No counterpart in the reference
+ * (which launches per instance); it serves the batching workload.
+ */
+size_t pf_batch_workspace(const pf_batch_instance* instances, int n);
+int pf_batch_prepare(const pf_batch_instance* instances, int n, void* workspace,
+                     size_t workspace_bytes, void* stream);
+int pf_batch_run(void* workspace, int64_t* stats, void* stream);
+int64_t* pf_batch_slab(void* workspace, int i);
+
 /* ---- seeded synthetic inputs (identical to the CPU generator) ------------ */
 /* config ids: 0 = small (250K x 1M, 25 groups), 1 = scale (150M x 600M,
  * 1.5M groups); `rows` and `lo` select rows [lo, lo + rows). */
@@ -231,6 +268,12 @@ int pf_gen_build(int config, uint64_t seed, int64_t n_build, int64_t n_groups, i
                  int64_t rows, int64_t* key, int32_t* group, void* stream);
 int pf_gen_probe(int config, uint64_t seed, int64_t n_build, int64_t lo, int64_t rows,
                  int64_t* fk, int64_t* price, int64_t* disc, void* stream);
+/* One batching instance's probe rows: FK ranks drawn from the Zipf table
+ * (nbins bins: edges[nbins+1] ranks, thr[nbins] cumulative thresholds, both
+ * device arrays), values in cents. */
+int pf_gen_batch_probe(uint64_t seed, int64_t n_build, int64_t lo, int64_t rows, int nbins,
+                       const int64_t* edges, const uint64_t* thr, int64_t* fk, int64_t* value,
+                       void* stream);
 
 #ifdef __cplusplus
 }

@@ -64,6 +64,8 @@ def lib():
                                          _c_i64, _c_i64, _c_i64, _c_i64,
                                          ctypes.c_int, _i64p, _i64p]
         L.or_expected_groups.restype = _c_i64
+        L.or_gen_batch_probe.argtypes = [ctypes.c_uint64, _c_i64, _c_i64, _c_i64, ctypes.c_int,
+                                         _i64p, _u64p, _i64p, _i64p]
         _lib = L
     return _lib
 
@@ -215,6 +217,16 @@ def gen_probe(config: int, seed: int, n_build: int, lo: int, rows: int):
     disc = np.empty(rows, np.int64)
     lib().or_gen_probe(config, seed, n_build, lo, rows, fk, price, disc)
     return fk, price, disc
+
+
+def gen_batch_probe(seed: int, n_build: int, lo: int, rows: int, edges, thr):
+    """One batching instance's probe rows (fk, value) from its Zipf table."""
+    fk = np.empty(rows, np.int64)
+    val = np.empty(rows, np.int64)
+    e = _a(edges)
+    t = np.ascontiguousarray(thr, dtype=np.uint64)
+    lib().or_gen_batch_probe(seed, n_build, lo, rows, t.shape[0], e, t, fk, val)
+    return fk, val
 
 
 def expected_groups(config: int, seed: int, n_build: int, n_groups: int,

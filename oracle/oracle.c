@@ -357,6 +357,14 @@ void or_gen_probe(int config, uint64_t seed, int64_t n_build, int64_t lo, int64_
                      &disc[i]);
 }
 
+/* The CPU twin of one batching instance's probe rows (synth.h). */
+void or_gen_batch_probe(uint64_t seed, int64_t n_build, int64_t lo, int64_t rows, int nbins,
+                        const int64_t* edges, const uint64_t* thr, int64_t* fk, int64_t* value) {
+  const pf_perm_t perm = pf_perm_make(seed, (uint64_t)n_build);
+  for (int64_t i = 0; i < rows; ++i)
+    pf_gen_batch_probe_row(seed, &perm, nbins, edges, thr, (uint64_t)(lo + i), &fk[i], &value[i]);
+}
+
 typedef struct {
   int config;
   uint64_t seed;

@@ -65,7 +65,20 @@ _SIGS = {
                             _vp]),
     "pf_gen_probe": (_int, [_int, ctypes.c_uint64, _i64, _i64, _i64, _vp, _vp, _vp,
                             _vp]),
+    "pf_gen_batch_probe": (_int, [ctypes.c_uint64, _i64, _i64, _i64, _int, _vp, _vp, _vp, _vp,
+                                  _vp]),
+    "pf_batch_workspace": (_sz, [_vp, _int]),
+    "pf_batch_prepare": (_int, [_vp, _int, _vp, _sz, _vp]),
+    "pf_batch_run": (_int, [_vp, _vp, _vp]),
+    "pf_batch_slab": (_vp, [_vp, _int]),
 }
+
+
+class BatchInstance(ctypes.Structure):
+    """pf_batch_instance (include/pageflow_b200.h)."""
+    _fields_ = [("build_key", _vp), ("build_group", _vp), ("n_build", _i64),
+                ("probe_fk", _vp), ("probe_value", _vp), ("n_probe", _i64),
+                ("group_min", _i64), ("n_groups", _i64)]
 
 _lib = None
 

@@ -32,6 +32,19 @@ __global__ void k_gen_probe(uint64_t seed, uint64_t n_build, int miss, long long
   }
 }
 
+__global__ void k_gen_batch_probe(uint64_t seed, pf_perm_t perm, int nbins,
+                                  const int64_t* __restrict__ edges,
+                                  const uint64_t* __restrict__ thr, long long lo, long long rows,
+                                  long long* __restrict__ fk, long long* __restrict__ value) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < rows;
+       i += (long long)gridDim.x * blockDim.x) {
+    int64_t f, v;
+    pf_gen_batch_probe_row(seed, &perm, nbins, edges, thr, (uint64_t)(lo + i), &f, &v);
+    fk[i] = f;
+    value[i] = v;
+  }
+}
+
 unsigned grid_for(long long rows) {
   const long long want = (rows + 255) / 256;
   const long long cap = (long long)sm_count() * 16;
@@ -57,6 +70,22 @@ extern "C" int pf_gen_build(int config, uint64_t seed, int64_t n_build, int64_t 
         seed, (uint64_t)n_build, (uint64_t)n_groups, perm, lo, rows, (long long*)key, group);
   }
   PF_LAUNCH("k_gen_build");
+  return ok();
+}
+
+extern "C" int pf_gen_batch_probe(uint64_t seed, int64_t n_build, int64_t lo, int64_t rows,
+                                  int nbins, const int64_t* edges, const uint64_t* thr,
+                                  int64_t* fk, int64_t* value, void* stream) {
+  if (n_build < 1 || lo < 0 || rows < 0 || nbins < 1)
+    return fail(PF_EINVAL, "gen_batch_probe: bad arguments");
+  if (rows == 0) return ok();
+  const pf_perm_t perm = pf_perm_make(seed, (uint64_t)n_build);
+  {
+    PF_KERNEL("k_gen_batch_probe", (cudaStream_t)stream);
+    k_gen_batch_probe<<<grid_for(rows), 256, 0, (cudaStream_t)stream>>>(
+        seed, perm, nbins, edges, thr, lo, rows, (long long*)fk, (long long*)value);
+  }
+  PF_LAUNCH("k_gen_batch_probe");
   return ok();
 }
 

@@ -125,4 +125,35 @@ PF_HD void pf_gen_probe_row(uint64_t seed, uint64_t n_build, int miss_per_10, ui
   *disc = (int64_t)pf_range(pf_u(seed, 5, r), 11);
 }
 
+/*
+ * The batching workload's probe rows (one instance, its own seed): the FK's
+ * rank among the instance's n_build keys follows a Zipf law, sampled with a
+ * table the host computes once per instance: nbins bins of ranks
+ * [edges[b], edges[b+1]) and cumulative probabilities thr[b] (scaled to
+ * 2^64, thr[nbins-1] = 2^64 - 1); the bin is the first whose threshold
+ * exceeds u, the rank uniform inside it.  Uniform FKs are one bin.  Integer
+ * only, so the CPU and the GPU draw the same rows.
+ *   fk = 1 + perm(rank)          (hot ranks land on scattered keys)
+ *   value = range(u(seed,5,r), 10^7)   cents
+ */
+PF_HD uint64_t pf_zipf_rank(uint64_t u_bin, uint64_t u_in, int nbins, const int64_t* edges,
+                            const uint64_t* thr) {
+  int lo = 0, hi = nbins - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (u_bin < thr[mid]) hi = mid;
+    else lo = mid + 1;
+  }
+  const uint64_t width = (uint64_t)(edges[lo + 1] - edges[lo]);
+  return (uint64_t)edges[lo] + pf_range(u_in, width);
+}
+
+PF_HD void pf_gen_batch_probe_row(uint64_t seed, const pf_perm_t* perm, int nbins,
+                                  const int64_t* edges, const uint64_t* thr, uint64_t r,
+                                  int64_t* fk, int64_t* value) {
+  const uint64_t rank = pf_zipf_rank(pf_u(seed, 3, r), pf_u(seed, 4, r), nbins, edges, thr);
+  *fk = (int64_t)(1 + pf_perm(perm, rank));
+  *value = (int64_t)pf_range(pf_u(seed, 5, r), 10000000);
+}
+
 #endif /* PF_SYNTH_H */

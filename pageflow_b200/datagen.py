@@ -14,6 +14,7 @@ from __future__ import annotations
 
 from dataclasses import dataclass
 
+import numpy as np
 import torch
 
 from . import _native as N
@@ -51,6 +52,81 @@ def gen_build(w: Workload, device, lo: int = 0, rows: int | None = None):
                                      key.data_ptr(), grp.data_ptr(), N.stream_of(device)),
                 "gen_build")
     return key, grp
+
+
+@dataclass(frozen=True)
+class BatchSpec:
+    """One instance of the batching workload (sizes drawn on the host from
+    the workload seed, so the CPU oracle and the GPU draw the same rows)."""
+    index: int
+    seed: int           # the instance's own generator seed
+    n_build: int        # unique keys, a permutation of 1..n_build
+    n_probe: int
+    skew: float         # Zipf exponent of the probe FKs over the build keys
+    n_groups: int
+    edges: np.ndarray   # Zipf table: bin b holds ranks [edges[b], edges[b+1])
+    thr: np.ndarray     # cumulative bin probabilities scaled to 2^64 (uint64)
+
+
+def zipf_table(n: int, s: float, bins: int = 256):
+    """Geometric rank bins over [0, n) and their cumulative Zipf(s) masses
+    (the integral of x^-s over each bin's ranks 1-based), as uint64
+    thresholds; one bin for s = 0."""
+    if s == 0.0 or n <= 1:
+        return np.array([0, n], np.int64), np.array([np.iinfo(np.uint64).max], np.uint64)
+    e = np.unique(np.floor(np.geomspace(1, n + 1, bins + 1)).astype(np.int64))
+    e[0], e[-1] = 1, n + 1
+    e = np.unique(e)
+    lo, hi = e[:-1].astype(np.float64), e[1:].astype(np.float64)
+    if abs(s - 1.0) < 1e-12:
+        mass = np.log(hi) - np.log(lo)
+    else:
+        mass = (hi ** (1 - s) - lo ** (1 - s)) / (1 - s)
+    cdf = np.cumsum(mass) / mass.sum()
+    # the largest double below 2^64 is 2^64 - 2048; the last bin takes the rest
+    thr = np.minimum(np.floor(cdf * 2.0 ** 64), 2.0 ** 64 - 2048.0)
+    thr_u = np.array([int(x) for x in thr], dtype=np.uint64)
+    thr_u = np.maximum.accumulate(thr_u)
+    thr_u[-1] = np.iinfo(np.uint64).max
+    return (e - 1).astype(np.int64), thr_u
+
+
+def batch_workload(n_inst: int = 4096, seed: int = 3, build_range=(1_000, 4_000_000),
+                   group_range=(4, 1_000_000), ratio_range=(4, 16), skews=(0.0, 0.8, 1.2)):
+    """The batching workload: build sizes log-uniform in build_range, probe
+    sizes 4-16x build, FK skew per instance from Zipf s in skews, group
+    cardinality log-uniform in group_range, values in int64 cents."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_inst):
+        nb = int(round(float(np.exp(rng.uniform(np.log(build_range[0]), np.log(build_range[1]))))))
+        ratio = int(rng.integers(ratio_range[0], ratio_range[1] + 1))
+        s = float(skews[int(rng.integers(0, len(skews)))])
+        ng = int(round(float(np.exp(rng.uniform(np.log(group_range[0]), np.log(group_range[1]))))))
+        edges, thr = zipf_table(nb, s)
+        out.append(BatchSpec(i, seed * 1_000_003 + i, nb, nb * ratio, s, ng, edges, thr))
+    return out
+
+
+def gen_batch_instance(spec: BatchSpec, device):
+    """(build_key, build_group, probe_fk, probe_value) of one instance on the
+    device."""
+    key = torch.empty(spec.n_build, dtype=torch.int64, device=device)
+    grp = torch.empty(spec.n_build, dtype=torch.int32, device=device)
+    fk = torch.empty(spec.n_probe, dtype=torch.int64, device=device)
+    val = torch.empty(spec.n_probe, dtype=torch.int64, device=device)
+    edges = torch.from_numpy(spec.edges).to(device)
+    thr = torch.from_numpy(spec.thr.view(np.int64)).to(device)
+    L = N.lib()
+    with torch.cuda.device(device):
+        st = N.stream_of(device)
+        N.check(L.pf_gen_build(1, spec.seed, spec.n_build, spec.n_groups, 0, spec.n_build,
+                               key.data_ptr(), grp.data_ptr(), st), "gen_build")
+        N.check(L.pf_gen_batch_probe(spec.seed, spec.n_build, 0, spec.n_probe, thr.numel(),
+                                     edges.data_ptr(), thr.data_ptr(), fk.data_ptr(),
+                                     val.data_ptr(), st), "gen_batch_probe")
+    torch.cuda.current_stream(device).synchronize()
+    return key, grp, fk, val
 
 
 def gen_probe(w: Workload, device, lo: int = 0, rows: int | None = None):
