@@ -521,6 +521,189 @@ def run_batch(args, world, rank, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def paged_kept_rows(spec) -> int:
+    """Rows of the paged table whose date passes the filter, from the date
+    column's closed form (date = 8035 + ((r mod 2^20) * 2557) >> 20)."""
+    import numpy as np
+    cyc = 1 << 20
+    d = 8035 + ((np.arange(cyc, dtype=np.int64) * 2557) >> 20)
+    ok = (d >= spec.date_lo) & (d < spec.date_hi)
+    full, rest = divmod(spec.n_rows, cyc)
+    return int(ok.sum()) * full + int(ok[:rest].sum())
+
+
+def h2d_peak_gbs(dev, nbytes=2 << 30) -> float:
+    """A plain pinned host -> device copy's rate on this box (best of 5)."""
+    import torch
+    src = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    dst = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dst.copy_(src, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, nbytes / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    del src, dst
+    return best
+
+
+def run_paged(args, world, rank, local_rank):
+    """The paged workload (seed 2): 2.4B rows x 6 columns as PFC1 pages in
+    pinned host memory (generated and encoded on the host, untimed); a step
+    is one decode -> date filter -> radix partition pass over the whole
+    table, the compressed pages crossing the link inside the timed region.
+    Reports the effective uncompressed link rate (raw table bytes / s), the
+    compressed link rate against a plain pinned copy's, and HBM bytes / s."""
+    import numpy as np
+    import torch
+    import oracle
+    from pageflow_b200 import _native, paged
+
+    name = args.workload
+    spec = paged.PAGED
+    if "/" in name:
+        spec = paged.scaled(spec, float(name.split("/", 1)[1]))
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    t0 = time.perf_counter()
+    table = paged.PagedTable.generate(spec)
+    gen_s = time.perf_counter() - t0
+    kept = paged_kept_rows(spec)
+    B = args.B or 256
+    gpb = 64
+    scan = paged.PagedScan(table, "date", spec.date_lo, spec.date_hi, "fk", B=B,
+                           groups_per_batch=gpb,
+                           capacity_rows=kept + spec.rows_per_page * gpb)
+    for _ in range(args.warmup):
+        parts = scan.run()
+    torch.cuda.synchronize()
+    st = parts.read_stats()
+    offs = parts.bucket_offsets.cpu().numpy()
+    # checks: the kept rows (closed form), the batch totals, and a sample of
+    # rows in their buckets (oracle mix64)
+    ok_rows = st["rows"] == kept and int(offs[:, B].sum()) == kept and st["bad_pages"] == 0
+    k = offs.shape[0] // 2
+    lo_r, hi_r = int(offs[k, 0]), int(offs[k, 0] + offs[k, B])
+    fk = parts.columns["fk"][lo_r:hi_r].cpu().numpy()
+    bk = oracle.bucket(fk, B)
+    want = np.repeat(np.arange(B), np.diff(np.append(offs[k, :B], offs[k, 0] + offs[k, B])))
+    ok_buckets = bool(np.array_equal(bk, want))
+
+    sampler = ClockSampler(None)
+    time.sleep(0.3)
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = _native.launch_count()
+    _native.profile_begin()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        scan.run()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    prof = _native.profile_end()
+    launches = _native.launch_count() - launches0
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+
+    # end to end: the same pass plus the bucket offsets and counters read back
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        p = scan.run()
+        offs_h = p.bucket_offsets.to("cpu", non_blocking=True)
+        st_h = p.stats.to("cpu", non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
+    d2h = offs_h.numel() * 8 + st_h.numel() * 8
+
+    peak, peak_kind = measured_peak()
+    link_peak = h2d_peak_gbs(dev)
+    comp = table.total_bytes
+    raw = table.raw_bytes
+    out_bytes = kept * (8 + 8 + 8 + 4 + 4)
+    hbm_alg = 2 * comp + out_bytes      # pages land once and are read once; rows written once
+    kernels = {n: {"ms_per_step": v[0] / args.steps, "launches_per_step": v[1] / args.steps}
+               for n, v in prof.items()}
+    scat = prof.get("k_paged_scatter")
+    roofline = None
+    if scat:
+        per_launch_ms = scat[0] / scat[1]
+        n_launch_step = scat[1] / args.steps
+        # the scatter reads every page of the batch and writes the kept rows
+        alg_launch = (comp + out_bytes) / n_launch_step
+        ach = alg_launch / (per_launch_ms / 1e3) / 1e9
+        roofline = {"bound": "hbm", "kernel": "k_paged_scatter", "achieved": ach, "peak": peak,
+                    "unit": "GB/s", "frac": ach / peak, "traffic": None,
+                    "bytes_per_launch": alg_launch, "peak_source": peak_kind}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = paged_cpu_baseline(table, spec)
+    if rank == 0:
+        line = {
+            "metric": "paged scan effective link GB/s (uncompressed bytes / s)",
+            "value": world * raw / (ms / 1e3) / 1e9, "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int64/int32", "data": "synthetic (seeded generator, PFC1 pages in "
+                                            "pinned host memory)",
+            "config": {"workload": name, "rows": spec.n_rows, "columns": list(table.names),
+                       "rows_per_page": spec.rows_per_page, "groups_per_batch": gpb,
+                       "fanout_B": B, "filter": f"{spec.date_lo} <= date < {spec.date_hi}",
+                       "kept_rows": kept, "raw_bytes": raw, "compressed_bytes": comp,
+                       "ratio": raw / comp, "generate_s": gen_s,
+                       "l2": "pages stream from the host: every step is cold"},
+            "rows_per_s": world * spec.n_rows / (ms / 1e3),
+            "link": {"compressed_gbs": comp / (ms / 1e3) / 1e9, "h2d_copy_peak_gbs": link_peak,
+                     "frac": comp / (ms / 1e3) / 1e9 / link_peak},
+            "hbm": {"algorithmic_bytes": hbm_alg, "gbs": hbm_alg / (ms / 1e3) / 1e9,
+                    "peak": peak, "frac": hbm_alg / (ms / 1e3) / 1e9 / peak},
+            "roofline": roofline, "kernels": kernels,
+            "checks": {"kept_rows": ok_rows, "buckets_sample": ok_buckets, "stats": st},
+            "e2e": {"value": world * raw / (e2e_ms / 1e3) / 1e9, "unit": "GB/s",
+                    "h2d_bytes_per_step": comp, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": e2e_ms},
+            "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def paged_cpu_baseline(table, spec, seconds: float = 10.0):
+    """The oracle's decode -> filter -> partition on every host thread over
+    the table's first row groups (about `seconds` of work): decoded bytes /
+    s, uncompressed."""
+    import numpy as np
+    from concurrent.futures import ThreadPoolExecutor
+    import oracle
+    threads = oracle.threads()
+    pages = table.pages.numpy()
+    ends = np.append(table.directory[1:], table.total_bytes)
+    nc = len(table.names)
+    fc, kc = table.names.index("date"), table.names.index("fk")
+
+    def group(g):
+        cols = [oracle.page_decode(pages[table.directory[g * nc + c]:ends[g * nc + c]])
+                for c in range(nc)]
+        keep = (cols[fc] >= spec.date_lo) & (cols[fc] < spec.date_hi)
+        bk = oracle.bucket(cols[kc][keep], 256)
+        order = np.argsort(bk, kind="stable")
+        return [c[keep][order] for i, c in enumerate(cols) if i != fc]
+
+    done, t0 = 0, time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        while time.perf_counter() - t0 < seconds and done < table.n_groups:
+            n = min(threads, table.n_groups - done)
+            list(ex.map(group, range(done, done + n)))
+            done += n
+    el = time.perf_counter() - t0
+    rows = min(table.n_rows, done * table.rows_per_page)
+    raw = rows * sum(table.esizes)
+    return {"value": raw / el / 1e9, "unit": "GB/s", "cores": threads, "kind": "port",
+            "sample": f"the first {done} row groups ({rows} rows), {el:.1f} s"}
+
+
 def main(argv=None) -> int:
     args = parse_args(argv)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -528,6 +711,15 @@ def main(argv=None) -> int:
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.workload == "batch":
         run_batch(args, world, rank, local_rank)
+        return 0
+    if args.workload.startswith("paged"):
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable":
+                                  "the paged workload's reference arm is the oracle decoder, "
+                                  "reported as cpu_baseline of --workload paged"}), flush=True)
+            return 0
+        run_paged(args, world, rank, local_rank)
         return 0
     w = workload(args.workload)
     if args.impl == "reference":

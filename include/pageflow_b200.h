@@ -224,6 +224,54 @@ int pf_groups_finish(const int64_t* sum, const int64_t* count, int64_t group_min
                      int64_t n_groups, int64_t* keys_out, int64_t* sums_out, int64_t* counts_out,
                      int64_t* host_out, void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- compressed pages: decode on arrival, filter, partition ---------------- */
+/*
+ * PFC1 pages (pageflow_b200/csrc/codec.h): a page holds up to 2^30 values of
+ * one int32/int64 column, encoded with the smallest of FOR bitpacking, DELTA
+ * + FOR, RLE (run values FOR or DELTA, run ends DELTA) or RAW, in
+ * independently decodable 1024-value mini-blocks.  Replaces the reference's
+ * nvCOMP CASCADED codec (compression/nvcomp_manager.cu:162-173) with a format
+ * of our own.  pf_page_encode (host) writes one page into out; returns its
+ * bytes or a negative PF_E* code.
+ */
+int64_t pf_page_encode(const void* values, int esize, int64_t n, void* out, int64_t capacity);
+/*
+ * The paged benchmark's probe table generated and encoded on host threads:
+ * n_rows rows of 6 columns (fk int64 with Zipf ranks from the given table over
+ * n_build keys, date int32 sorted within 2^20-row runs in [8035, 10591],
+ * price int64, quantity int64, flag int32, status int32), rows_per_page rows
+ * a row group.  pf_paged_fetch copies the pages (group-major, columns in
+ * order) into dst and each page's byte offset into directory[n_groups * 6],
+ * and frees the handle.
+ */
+int pf_paged_generate(uint64_t seed, int64_t n_rows, int rows_per_page, int64_t n_build,
+                      const int64_t* zipf_edges, const uint64_t* zipf_thr, int nbins, int threads,
+                      void** handle, int64_t* total_bytes);
+int pf_paged_fetch(void* handle, void* dst, int64_t* directory, int64_t* n_groups);
+/*
+ * Decode on arrival: batches of groups_per_batch row groups are copied from
+ * pinned host pages (host_pages, total_bytes; directory as pf_paged_fetch
+ * writes it, host memory) to the device on a copy stream, NSTAGE batches
+ * ahead, while `stream` decodes each batch, keeps the rows with lo <=
+ * column[filter_col] < hi, and scatters their other columns into outs[c]
+ * (device, capacity_rows rows each; NULL to drop a column) by the key
+ * column's radix bucket (top log2(B) bits of mix64).  Each batch's rows form
+ * one region of the outputs, bucket after bucket: bucket_offsets (device,
+ * [n_batches][B + 1]) receives each bucket's first output row (-1 when the
+ * batch did not fit the capacity and was skipped) and the batch's rows.
+ * stats (device int64[4]): rows written, batches skipped, bad pages.  Queued
+ * only.  The pages are trusted input (written by pf_page_encode /
+ * pf_paged_generate).
+ */
+size_t pf_paged_scan_workspace(const int64_t* directory, int64_t n_groups, int ncols,
+                               int64_t total_bytes, int groups_per_batch, int B);
+int pf_paged_scan(const uint8_t* host_pages, const int64_t* directory, int64_t n_groups, int ncols,
+                  const int* esizes, int64_t total_bytes, int64_t n_rows, int rows_per_page,
+                  int filter_col, int64_t lo, int64_t hi, int key_col, int B,
+                  int groups_per_batch, void* const* outs, int64_t capacity_rows,
+                  int64_t* bucket_offsets, int64_t* stats, void* workspace,
+                  size_t workspace_bytes, void* stream);
+
 /* ---- batched join -> group-by (many uneven instances, one launch) --------- */
 /*
  * One instance: SELECT group, SUM(value), COUNT(*) FROM build JOIN probe ON

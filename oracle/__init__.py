@@ -66,6 +66,11 @@ def lib():
         L.or_expected_groups.restype = _c_i64
         L.or_gen_batch_probe.argtypes = [ctypes.c_uint64, _c_i64, _c_i64, _c_i64, ctypes.c_int,
                                          _i64p, _u64p, _i64p, _i64p]
+        _u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+        L.or_page_decode.argtypes = [_u8p, _c_i64, _i64p, _c_i64]
+        L.or_page_decode.restype = _c_i64
+        L.or_gen_paged.argtypes = [ctypes.c_uint64, _c_i64, ctypes.c_int, _i64p, _u64p,
+                                   _c_i64, _c_i64] + [_i64p] * 6
         _lib = L
     return _lib
 
@@ -240,3 +245,59 @@ def expected_groups(config: int, seed: int, n_build: int, n_groups: int,
     if m < 0:
         raise MemoryError("or_expected_groups")
     return s, c, int(m)
+
+
+# ---- compressed pages ------------------------------------------------------
+
+def page_decode(page) -> np.ndarray:
+    """The values of one PFC1 page (int64; int32 columns sign-extended).
+    Raises ValueError for a malformed page."""
+    if isinstance(page, np.ndarray):
+        b = np.ascontiguousarray(page, dtype=np.uint8)
+    else:
+        b = np.frombuffer(bytes(page), np.uint8)
+    n = int(b[8:12].view(np.uint32)[0]) if b.shape[0] >= 12 else 0
+    out = np.empty(max(n, 1), np.int64)
+    got = lib().or_page_decode(b, b.shape[0], out, out.shape[0])
+    if got < 0:
+        raise ValueError(f"malformed page (status {got})")
+    return out[:got]
+
+
+PAGED_COLUMNS = ("fk", "date", "price", "quantity", "flag", "status")
+
+
+def gen_paged(seed: int, n_build: int, lo: int, rows: int, edges, thr):
+    """Rows [lo, lo + rows) of the paged workload's 6 columns (int64 each)."""
+    cols = [np.empty(rows, np.int64) for _ in PAGED_COLUMNS]
+    e = _a(edges)
+    t = np.ascontiguousarray(thr, dtype=np.uint64)
+    lib().or_gen_paged(seed, n_build, t.shape[0], e, t, lo, rows, *cols)
+    return dict(zip(PAGED_COLUMNS, cols))
+
+
+def paged_scan(cols: dict, n_rows: int, rows_per_page: int, groups_per_batch: int,
+               filter_col: str, lo: int, hi: int, key_col: str, B: int):
+    """The decode -> range filter -> radix partition of a paged table, per
+    batch of groups_per_batch row groups: for each batch, the per-bucket row
+    counts and each kept column's rows in bucket order (stable within a
+    bucket; the product's order within a bucket is unspecified).  Follows
+    IO/transfer/pre_comp_stage.py:54-73 (mask compaction), operators/
+    filter.py:10-16 (the range mask) and the partition of
+    tests/operators/test_partition_sort.py:106-118."""
+    rows_b = rows_per_page * groups_per_batch
+    out = []
+    for r0 in range(0, n_rows, rows_b):
+        r1 = min(n_rows, r0 + rows_b)
+        f = cols[filter_col][r0:r1]
+        keep = (f >= lo) & (f < hi)
+        keys = cols[key_col][r0:r1][keep]
+        bk = bucket(keys, B)
+        order = np.argsort(bk, kind="stable")
+        counts = np.bincount(bk, minlength=B).astype(np.int64)
+        batch = {"counts": counts}
+        for name, v in cols.items():
+            if name != filter_col:
+                batch[name] = v[r0:r1][keep][order]
+        out.append(batch)
+    return out

@@ -432,3 +432,123 @@ int64_t or_expected_groups(int config, uint64_t seed, int64_t n_build, int64_t n
   free(th);
   return matched;
 }
+
+/* ---- compressed pages ------------------------------------------------------ */
+/*
+ * A PFC1 page decoder restated from the format's definition (the page header,
+ * stream header and block table of pageflow_b200/csrc/codec.h), independent of
+ * the product's decoder: fields are read byte by byte and bit fields bit by
+ * bit.  It stands for the decode half of the reference's codec binding
+ * (compression/nvcomp_manager.cu:679 mgr_decompress of the CASCADED codec
+ * configured at :162-173): a page decodes to exactly the values encoded.
+ */
+static uint64_t rd_u(const uint8_t* p, int bytes) {
+  uint64_t x = 0;
+  for (int i = 0; i < bytes; ++i) x |= (uint64_t)p[i] << (8 * i);
+  return x;
+}
+
+static uint64_t rd_bits(const uint8_t* words, uint64_t j, uint32_t bw) {
+  uint64_t v = 0;
+  for (uint32_t b = 0; b < bw; ++b) {
+    const uint64_t bit = j * bw + b;
+    v |= (uint64_t)((words[bit >> 3] >> (bit & 7)) & 1u) << b;
+  }
+  return v;
+}
+
+/* One FOR / DELTA stream at byte offset off of a page of `bytes`; n values
+ * expected.  Returns 0, or -1 when the stream is malformed. */
+static int decode_stream(const uint8_t* page, uint64_t bytes, uint64_t off, uint64_t n,
+                         int64_t* out) {
+  if (off + 16 > bytes) return -1;
+  const uint32_t scheme = (uint32_t)rd_u(page + off, 4);
+  const uint64_t sn = rd_u(page + off + 4, 4), nblk = rd_u(page + off + 8, 4);
+  if ((scheme != 1 && scheme != 2) || sn != n || nblk != (n + 1023) / 1024) return -1;
+  const uint64_t tab = off + 16, words = tab + 32 * nblk;
+  if (words > bytes) return -1;
+  for (uint64_t k = 0; k < nblk; ++k) {
+    const uint8_t* b = page + tab + 32 * k;
+    const uint64_t base = rd_u(b, 8), first = rd_u(b + 8, 8);
+    const uint64_t woff = rd_u(b + 16, 4), bw = rd_u(b + 20, 4);
+    if (bw > 64) return -1;
+    const uint64_t cnt = n - 1024 * k < 1024 ? n - 1024 * k : 1024;
+    if (words + 4 * woff + (bw * cnt + 7) / 8 > bytes) return -1;
+    uint64_t prev = 0;
+    for (uint64_t j = 0; j < cnt; ++j) {
+      const uint64_t field = base + rd_bits(page + words + 4 * woff, j, (uint32_t)bw);
+      uint64_t v;
+      if (scheme == 1) v = field;
+      else v = j == 0 ? first : prev + field;
+      out[1024 * k + j] = (int64_t)v;
+      prev = v;
+    }
+  }
+  return 0;
+}
+
+/* Decodes the page at page[0, bytes) into out[0, capacity) as int64 (int32
+ * columns sign-extended).  Returns the page's rows, or -1 for a malformed
+ * page, -2 when capacity is short. */
+int64_t or_page_decode(const uint8_t* page, int64_t bytes, int64_t* out, int64_t capacity) {
+  if (bytes < 64 || rd_u(page, 4) != 0x31434650u) return -1;
+  const int scheme = page[4], esize = page[5];
+  const uint64_t n = rd_u(page + 8, 4), nruns = rd_u(page + 12, 4);
+  const uint64_t s0 = rd_u(page + 16, 4), s1 = rd_u(page + 20, 4), pb = rd_u(page + 24, 4);
+  if ((esize != 4 && esize != 8) || pb > (uint64_t)bytes || pb % 16) return -1;
+  if ((int64_t)n > capacity) return -2;
+  if (scheme == 0) {
+    if (s0 + n * (uint64_t)esize > pb) return -1;
+    for (uint64_t i = 0; i < n; ++i) {
+      const uint64_t x = rd_u(page + s0 + i * esize, esize);
+      out[i] = esize == 8 ? (int64_t)x : (int64_t)(int32_t)(uint32_t)x;
+    }
+    return (int64_t)n;
+  }
+  if (scheme == 1 || scheme == 2) {
+    if (decode_stream(page, pb, s0, n, out)) return -1;
+  } else if (scheme == 3) {
+    if (nruns == 0 || nruns > 4096 || nruns > n) return -1;
+    int64_t* v = (int64_t*)malloc(sizeof(int64_t) * nruns);
+    int64_t* e = (int64_t*)malloc(sizeof(int64_t) * nruns);
+    int bad = !v || !e || decode_stream(page, pb, s0, nruns, v) ||
+              decode_stream(page, pb, s1, nruns, e);
+    int64_t row = 0;
+    for (uint64_t r = 0; !bad && r < nruns; ++r) {
+      if (e[r] <= row || e[r] > (int64_t)n) {
+        bad = 1;
+        break;
+      }
+      for (; row < e[r]; ++row) out[row] = v[r];
+    }
+    if (!bad && row != (int64_t)n) bad = 1;
+    free(v);
+    free(e);
+    if (bad) return -1;
+  } else {
+    return -1;
+  }
+  if (esize == 4)
+    for (uint64_t i = 0; i < n; ++i) out[i] = (int64_t)(int32_t)(uint32_t)(uint64_t)out[i];
+  return (int64_t)n;
+}
+
+/* The CPU twin of the paged workload's probe table (pageflow_b200/csrc/
+ * codec.cu), rows [lo, lo + rows) of its 6 columns as int64: fk (Zipf rank
+ * over n_build keys through the key permutation), date (sorted within
+ * 2^20-row runs over [8035, 10591]), price, quantity, flag, status. */
+void or_gen_paged(uint64_t seed, int64_t n_build, int nbins, const int64_t* edges,
+                  const uint64_t* thr, int64_t lo, int64_t rows, int64_t* fk, int64_t* date,
+                  int64_t* price, int64_t* qty, int64_t* flag, int64_t* status) {
+  const pf_perm_t perm = pf_perm_make(seed, (uint64_t)n_build);
+  for (int64_t i = 0; i < rows; ++i) {
+    const uint64_t r = (uint64_t)(lo + i);
+    const uint64_t rank = pf_zipf_rank(pf_u(seed, 2, r), pf_u(seed, 3, r), nbins, edges, thr);
+    fk[i] = (int64_t)(1 + pf_perm(&perm, rank));
+    date[i] = 8035 + (int64_t)(((r % (1u << 20)) * 2557u) / (1u << 20));
+    price[i] = 90000 + (int64_t)pf_range(pf_u(seed, 4, r), 10410001);
+    qty[i] = 1 + (int64_t)pf_range(pf_u(seed, 5, r), 50);
+    flag[i] = (int64_t)pf_range(pf_u(seed, 6, r), 3);
+    status[i] = (int64_t)pf_range(pf_u(seed, 7, r), 2);
+  }
+}

@@ -67,6 +67,13 @@ _SIGS = {
                             _vp]),
     "pf_gen_batch_probe": (_int, [ctypes.c_uint64, _i64, _i64, _i64, _int, _vp, _vp, _vp, _vp,
                                   _vp]),
+    "pf_page_encode": (_i64, [_vp, _int, _i64, _vp, _i64]),
+    "pf_paged_generate": (_int, [ctypes.c_uint64, _i64, _int, _i64, _vp, _vp, _int, _int,
+                                 ctypes.POINTER(_vp), ctypes.POINTER(_i64)]),
+    "pf_paged_fetch": (_int, [_vp, _vp, _vp, ctypes.POINTER(_i64)]),
+    "pf_paged_scan_workspace": (_sz, [_vp, _i64, _int, _i64, _int, _int]),
+    "pf_paged_scan": (_int, [_vp, _vp, _i64, _int, _vp, _i64, _i64, _int, _int, _i64, _i64,
+                             _int, _int, _int, _vp, _i64, _vp, _vp, _vp, _sz, _vp]),
     "pf_batch_workspace": (_sz, [_vp, _int]),
     "pf_batch_prepare": (_int, [_vp, _int, _vp, _sz, _vp]),
     "pf_batch_run": (_int, [_vp, _vp, _vp]),
