@@ -374,7 +374,7 @@ extern "C" int pf_join_unique_hash(const int64_t* build0, const int64_t* build1,
   const long long* p1 = (const long long*)(nkeys == 2 ? probe1 : probe0);
   if (nkeys == 2) {
     {
-      PF_KERNEL("k_uh_build", 0);
+      PF_KERNEL("k_uh_build", st);
       k_uh_build<true><<<blocks_for(n_build, T), T, 0, st>>>(b0, b1, n_build, l.table, logcap);
     }
     {
@@ -383,7 +383,7 @@ extern "C" int pf_join_unique_hash(const int64_t* build0, const int64_t* build1,
     }
   } else {
     {
-      PF_KERNEL("k_uh_build", 0);
+      PF_KERNEL("k_uh_build", st);
       k_uh_build<false><<<blocks_for(n_build, T), T, 0, st>>>(b0, b1, n_build, l.table, logcap);
     }
     {
@@ -448,7 +448,7 @@ extern "C" int pf_join_semi_anti(const int64_t* build_key, int64_t n_build,
   host_out[0] = 0;
   host_out[1] = 0;  // the build below sets it through the alias
   {
-    PF_KERNEL("k_set_build", 0);
+    PF_KERNEL("k_set_build", st);
     k_set_build<<<blocks_for(n_build, T), T, 0, st>>>((const long long*)build_key,
                                                       (const long long*)build_val, n_build, l.table,
                                                       l.mn, l.mx, logcap, host_dev + 1);
@@ -540,7 +540,7 @@ extern "C" int pf_join_expand(const int64_t* sorted_ids, const int64_t* start, c
                 a.used);
   const long long threads = (n_pairs + EITEMS - 1) / EITEMS;
   {
-    PF_KERNEL("k_expand", 0);
+    PF_KERNEL("k_expand", st);
     k_expand<<<blocks_for(threads, T), T, 0, st>>>((const long long*)sorted_ids,
                                                    (const long long*)start, (const long long*)len,
                                                    l.incl, m, n_pairs, (long long*)cs,
