@@ -121,6 +121,25 @@ int pf_join_unique_hash(const int64_t* build0, const int64_t* build1, int64_t n_
                         const int64_t* probe0, const int64_t* probe1, int64_t n_probe, int nkeys,
                         int64_t* build_idx, int64_t* probe_idx, int64_t* host_out,
                         void* workspace, size_t workspace_bytes, void* stream);
+/*
+ * No counterpart in the reference.  pf_join_unique_hash for callers that may
+ * not allocate: no workspace argument and no device allocation by the
+ * library; its scratch is one fixed device array of
+ * PF_UH_STATIC_SCRATCH_BYTES (8 MiB + 64 KiB) inside the library, enough for
+ * 262144 build rows with 1048576 probe rows (the table takes 16 bytes per
+ * build row rounded up to a power of two, the partners 4 bytes per probe
+ * row).  Larger calls return PF_EINVAL before anything is queued.  The match
+ * count goes to match_count (device int64[1]) on the stream; nothing waits.
+ * The first call on a device, with that device current, sets the scratch up
+ * (looks up its device address, loading the library's module there); make
+ * it before any stream capture.  The scratch is shared per device: calls
+ * that overlap on one device (two streams, two host threads) race.
+ */
+#define PF_UH_STATIC_SCRATCH_BYTES ((8u << 20) + (64u << 10))
+int pf_join_unique_hash_static(const int64_t* build0, const int64_t* build1, int64_t n_build,
+                               const int64_t* probe0, const int64_t* probe1, int64_t n_probe,
+                               int nkeys, int64_t* build_idx, int64_t* probe_idx,
+                               int64_t* match_count, void* stream);
 
 /* Residual operators of a semi/anti summary, as build.v OP probe.v. */
 #define PF_OP_NONE 0

@@ -18,6 +18,7 @@
 // writes its row count into the caller's pinned host_out through the device
 // alias, and waits for that count once.
 #include <climits>
+#include <mutex>
 
 #include "scan.cuh"
 
@@ -547,5 +548,122 @@ extern "C" int pf_join_expand(const int64_t* sorted_ids, const int64_t* start, c
                                                    (long long*)cr);
   }
   PF_LAUNCH("k_expand");
+  return ok();
+}
+
+// ---- unique hash join on static scratch (allocates nothing) -------------------
+//
+// pf_join_unique_hash with its scratch (hash table, per-row partners, per-block
+// counts) in one file-scope device array instead of a caller's workspace, and
+// its match count left on the device instead of a host wait.  The first call
+// on a device, with that device current, looks the array's address up once
+// (cudaGetSymbolAddress, which also loads this module on that device); later
+// calls reuse it.  The array is shared: calls that overlap on one device, from
+// two streams or two host threads, race on it.
+
+namespace pf {
+namespace {
+
+__device__ __align__(256) unsigned char g_uh_static_scratch[PF_UH_STATIC_SCRATCH_BYTES];
+
+constexpr int MAX_DEVICES = 64;
+std::mutex g_uh_static_mu;
+void* g_uh_static_ptr[MAX_DEVICES];
+
+// This device's address of g_uh_static_scratch (looked up on first use).
+int uh_static_scratch(void** out) {
+  int dev = 0;
+  PF_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= MAX_DEVICES)
+    return fail(PF_EDEVICE, "join_unique_hash_static: device %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_uh_static_mu);
+  if (!g_uh_static_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t rc = cudaGetSymbolAddress(&p, g_uh_static_scratch);
+    if (rc != cudaSuccess || !p)
+      return fail(PF_ECUDA, "join_unique_hash_static: cudaGetSymbolAddress: %s",
+                  cudaGetErrorString(rc));
+    g_uh_static_ptr[dev] = p;
+  }
+  *out = g_uh_static_ptr[dev];
+  return PF_OK;
+}
+
+}  // namespace
+}  // namespace pf
+
+extern "C" int pf_join_unique_hash_static(const int64_t* build0, const int64_t* build1,
+                                          int64_t n_build, const int64_t* probe0,
+                                          const int64_t* probe1, int64_t n_probe, int nkeys,
+                                          int64_t* build_idx, int64_t* probe_idx,
+                                          int64_t* match_count, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (nkeys != 1 && nkeys != 2)
+    return fail(PF_EINVAL, "join_unique_hash_static: one or two keys, got %d", nkeys);
+  if (n_build < 1 || n_probe < 1)
+    return fail(PF_EINVAL, "join_unique_hash_static: unique hash needs rows on both sides");
+  if (!build0 || !probe0 || (nkeys == 2 && (!build1 || !probe1)) || !build_idx || !probe_idx ||
+      !match_count)
+    return fail(PF_EINVAL, "join_unique_hash_static: null pointer");
+  // the sizes must fit the fixed scratch (checked before anything is queued)
+  if (n_build > PF_JOIN_MAX_ROWS || n_probe > PF_JOIN_MAX_ROWS)
+    return fail(PF_EINVAL, "join_unique_hash_static: at most %lld rows a side",
+                (long long)PF_JOIN_MAX_ROWS);
+  Arena need(nullptr, 0);
+  uh_layout(need, n_build, n_probe);
+  if (need.used > (size_t)PF_UH_STATIC_SCRATCH_BYTES)
+    return fail(PF_EINVAL,
+                "join_unique_hash_static: %lld build x %lld probe rows need %zu bytes of "
+                "scratch, the static scratch holds %zu (e.g. up to 262144 build with "
+                "1048576 probe rows); use pf_join_unique_hash",
+                (long long)n_build, (long long)n_probe, need.used,
+                (size_t)PF_UH_STATIC_SCRATCH_BYTES);
+  void* scratch = nullptr;
+  if (int rc = uh_static_scratch(&scratch)) return rc;
+  Arena a(scratch, PF_UH_STATIC_SCRATCH_BYTES);
+  UhLayout l = uh_layout(a, n_build, n_probe);
+  const uint64_t cap = pow2_at_least((uint64_t)std::max<long long>(2 * n_build, 2));
+  const int logcap = log2_exact(cap);
+  // the table starts empty (all ones) every call; partners, block counts and
+  // the total are written in full before they are read
+  PF_CUDA(cudaMemsetAsync(l.table, 0xff, cap * sizeof(unsigned long long), st));
+  const unsigned nblk = blocks_for(n_probe, CB);
+  const long long* b0 = (const long long*)build0;
+  const long long* b1 = (const long long*)(nkeys == 2 ? build1 : build0);
+  const long long* p0 = (const long long*)probe0;
+  const long long* p1 = (const long long*)(nkeys == 2 ? probe1 : probe0);
+  if (nkeys == 2) {
+    {
+      PF_KERNEL("k_uh_build", st);
+      k_uh_build<true><<<blocks_for(n_build, T), T, 0, st>>>(b0, b1, n_build, l.table, logcap);
+    }
+    {
+      PF_KERNEL("k_uh_probe", st);
+      k_uh_probe<true><<<nblk, CT, 0, st>>>(b0, b1, p0, p1, n_probe, l.table, logcap, l.partner,
+                                            l.bcnt);
+    }
+  } else {
+    {
+      PF_KERNEL("k_uh_build", st);
+      k_uh_build<false><<<blocks_for(n_build, T), T, 0, st>>>(b0, b1, n_build, l.table, logcap);
+    }
+    {
+      PF_KERNEL("k_uh_probe", st);
+      k_uh_probe<false><<<nblk, CT, 0, st>>>(b0, b1, p0, p1, n_probe, l.table, logcap,
+                                             l.partner, l.bcnt);
+    }
+  }
+  PF_LAUNCH("k_uh_build/k_uh_probe");
+  {
+    PF_KERNEL("k_scan_counts", st);
+    k_scan_counts<<<1, 1024, 0, st>>>(l.bcnt, nblk, l.total, (long long*)match_count);
+  }
+  PF_LAUNCH("k_scan_counts");
+  {
+    PF_KERNEL("k_uh_emit", st);
+    k_uh_emit<<<nblk, CT, 0, st>>>(l.partner, n_probe, l.bcnt, (long long*)build_idx,
+                                   (long long*)probe_idx);
+  }
+  PF_LAUNCH("k_uh_emit");
   return ok();
 }

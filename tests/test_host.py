@@ -166,3 +166,18 @@ def test_slab_rejects_bad_specs_on_the_host():
         DenseAggregationSlab(5, 4, torch.int64, [], [], "cpu")
     with pytest.raises(ValueError, match="unsupported slab reduction"):
         DenseAggregationSlab(0, 4, torch.int64, [(torch.int64, ())], ["mean"], "cpu")
+
+
+def test_static_scratch_join_refuses_sizes_before_any_device_work():
+    # the size check runs on the host before the scratch is looked up, so it
+    # answers without a GPU; the pointers are never dereferenced
+    from pageflow_b200 import _native
+    L = _native.lib()
+    fake = ctypes.c_void_p(256)
+    for nb, npr in [(262144 + 1, 1048576), (524289, 10), (10, 4 * 1048576)]:
+        rc = L.pf_join_unique_hash_static(fake, None, nb, fake, None, npr, 1, fake, fake, fake,
+                                          None)
+        assert rc == _native.PF_EINVAL
+        assert b"static scratch" in L.pf_last_error()
+    rc = L.pf_join_unique_hash_static(fake, None, 10, fake, None, 10, 3, fake, fake, fake, None)
+    assert rc == _native.PF_EINVAL
