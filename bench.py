@@ -209,15 +209,15 @@ def algorithmic_bytes(w, B_rounds):
     columns each pass must read and write once.  k_fhist reads each side's
     keys; the scatters read the source columns and write the carried ones
     (build: key 8 + group 4; probe: fk 8 + value 8, from fk, price and
-    discount); the build and probe rounds read the partitioned sides once;
-    the finish reads the 16-byte slab and writes the groups it keeps."""
+    discount); the rounds (k_fround: build round r + 1 while probing round
+    r) read the partitioned sides once (build 12 B, probe 16 B a row); the
+    finish reads the 16-byte slab and writes the groups it keeps."""
     nb, npr, g = w.n_build, w.n_probe, w.n_groups
     return {
         "k_fhist": 8 * (nb + npr),
         "k_fscatter_build": nb * (12 + 12),
         "k_fscatter_probe": npr * (24 + 16),
-        "k_fbuild": nb * 12,
-        "k_fprobe": npr * 16,
+        "k_fround": nb * 12 + npr * 16,
         "k_gcount": g * 8,
         "k_gemit": g * 16 + g * 24,
     }
