@@ -59,6 +59,12 @@ def parse_args(argv=None):
                     help="batch workload: instances the reference path runs (0: the whole wave)")
     ap.add_argument("--cpu-sample", type=float, default=0.01,
                     help="fraction of the workload the CPU baseline joins per sample")
+    ap.add_argument("--serve-requests", type=int, default=400,
+                    help="serve workload: requests in the trace")
+    ap.add_argument("--serve-rates", default="50,100,200,400,800,1200,1600,2000",
+                    help="serve workload: offered rates (requests/s) of the sweep")
+    ap.add_argument("--serve-iter-rows", type=int, default=1 << 27,
+                    help="serve workload: probe rows one persistent launch takes")
     return ap.parse_args(argv)
 
 
@@ -704,6 +710,180 @@ def paged_cpu_baseline(table, spec, seconds: float = 10.0):
             "sample": f"the first {done} row groups ({rows} rows), {el:.1f} s"}
 
 
+def _plain_request(dims, fact, r):
+    """One serving request the reference's way: the range mask, mask
+    compaction, then the plain-form join + group-by on the GPU."""
+    import torch
+    from oracle import plain_form
+    s = slice(r.row0, r.row0 + r.n_rows)
+    d = fact.date[s]
+    keep = (d >= r.date_lo) & (d < r.date_hi)
+    fk = fact.fk[s][keep]
+    val = fact.value[s][keep]
+    if fk.numel() == 0:
+        e = torch.empty(0, dtype=torch.int64, device=fk.device)
+        return e, e, e
+    return plain_form.join_aggregate(dims.keys[r.dim], dims.groups[r.dim], fk, val,
+                                     torch.zeros_like(val), 1)
+
+
+def run_serve(args, world, rank, local_rank):
+    """The serving workload (seed 4): 8 resident dimensions (1e5 to 2e8
+    keys) with persistent hash tables, a resident 1e9-row fact pool, and a
+    trace of requests (probe rows log-uniform in [1e5, 1e9], selectivity
+    uniform in [1%, 50%]) replayed as Poisson arrivals at each rate of the
+    sweep, admitted by a 150 GB HBM budget and batched into persistent
+    launches.  Beside it the reference's plain form per request (service
+    times measured one by one, queued FIFO at the same arrivals)."""
+    import numpy as np
+    import torch
+    from pageflow_b200 import _native, serve
+
+    name = args.workload
+    spec = serve.SERVE if "/" not in name else serve.scaled(serve.SERVE,
+                                                            float(name.split("/", 1)[1]))
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    t0 = time.perf_counter()
+    dims = serve.Dimensions(spec, dev)
+    fact = serve.FactPool(spec, dev)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    n = args.serve_requests
+    trace = serve.make_requests(spec, n, seed=spec.seed + 1000 * rank)
+    rates = [float(x) for x in args.serve_rates.split(",")]
+    srv = serve.Server(dims, fact, spec.budget_bytes, dev, iter_rows=args.serve_iter_rows)
+
+    def fresh(rate):
+        out = []
+        arr = serve.poisson_arrivals(n, rate, seed=spec.seed) if rate > 0 else np.zeros(n)
+        for r, a in zip(trace, arr):
+            out.append(serve.Request(r.id, r.dim, r.row0, r.n_rows, r.date_lo, r.date_hi,
+                                     float(a)))
+        return out
+
+    # warm-up and the results every later run is checked against: a burst
+    for _ in range(max(1, args.warmup)):
+        burst = fresh(0)
+        srv.run(burst, keep_results=True)
+    ours = {r.id: r.result for r in burst}
+    sampler = ClockSampler(None)
+    launches0 = _native.launch_count()
+    sweep = []
+    for rate in rates:
+        reqs = fresh(rate)
+        run = srv.run(reqs, keep_results=False)
+        lat = run.latencies() * 1e3
+        span = max(r.t_done for r in reqs) - min(r.arrival for r in reqs)
+        sweep.append({"rate": rate, "p50_ms": float(np.percentile(lat, 50)),
+                      "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+                      "completed_per_s": n / span, "rows_per_s": run.rows / span,
+                      "launches": run.launches, "max_admitted": run.max_admitted,
+                      "wall_s": run.wall_s})
+    launches = _native.launch_count() - launches0
+    clocks = sampler.stop()
+    rows_total = sum(r.n_rows for r in trace)
+    del srv
+    torch.cuda.empty_cache()
+
+    # the plain form, one request at a time, each checked against ours
+    plain = None
+    from oracle import plain_form
+    if plain_form.available() and not args.no_plain_form:
+        svc = np.zeros(n)
+        same = True
+        for r in trace:
+            torch.cuda.synchronize()
+            a = time.perf_counter()
+            k, s, c = _plain_request(dims, fact, r)
+            torch.cuda.synchronize()
+            svc[r.id] = time.perf_counter() - a
+            mine = ours[r.id]
+            same &= bool(np.array_equal(k.cpu().numpy(), mine[0]) and
+                         np.array_equal(s.cpu().numpy(), mine[1]) and
+                         np.array_equal(c.cpu().numpy(), mine[2]))
+            del k, s, c
+        for entry in sweep:
+            lat = serve.lindley(serve.poisson_arrivals(n, entry["rate"], seed=spec.seed),
+                                svc[[r.id for r in trace]]) * 1e3
+            entry["plain_p50_ms"] = float(np.percentile(lat, 50))
+            entry["plain_p99_ms"] = float(np.percentile(lat, 99))
+        plain = {"rows_per_s": rows_total / svc.sum(), "service_ms_mean": svc.mean() * 1e3,
+                 "identical_results": same,
+                 "kind": "mask + compaction (torch) + the reference's compiled partition_sort / "
+                         "join_unique_hash + its torch group-by, one request at a time; "
+                         "latency = FIFO queue over the measured service times"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = serve_cpu_baseline(spec, dims, fact, trace)
+    top = sweep[-1]
+    # the knee: the highest rate still served as offered (completions keep up
+    # with the trace's realised arrival rate) with p99 within 10x of the
+    # lowest rate's
+    knee = None
+    base_p99 = sweep[0]["p99_ms"]
+    for e in sweep:
+        arr = serve.poisson_arrivals(n, e["rate"], seed=spec.seed)
+        offered = (n - 1) / (arr[-1] - arr[0])
+        e["offered_per_s"] = offered
+        if e["completed_per_s"] >= 0.95 * offered and e["p99_ms"] <= 10 * base_p99:
+            knee = e["rate"]
+    res_bytes = float(np.mean([24 * ours[i][0].shape[0] for i in ours]))
+    if rank == 0:
+        line = {
+            "metric": "serving rows/s at the highest offered rate; p50/p99 latency per rate",
+            "value": world * top["rows_per_s"], "unit": "rows/s", "n_gpus": world,
+            "steps": n, "warmup": args.warmup, "ms_per_step": 1e3 / top["completed_per_s"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int64", "data": "synthetic (seeded generator, resident on the device)",
+            "config": {"workload": name, "requests": n, "rates": rates,
+                       "dims_keys": list(spec.dim_keys), "dims_groups": list(spec.dim_groups),
+                       "fact_rows": spec.fact_rows, "budget_gb": spec.budget_bytes / 1e9,
+                       "iter_rows": args.serve_iter_rows, "trace_rows": rows_total,
+                       "setup_s": setup_s,
+                       "l2": "requests scan slices of a 20 GB fact pool, far above L2"},
+            "sweep": sweep, "knee_rate": knee, "plain_form": plain,
+            "e2e": {"value": world * top["rows_per_s"], "unit": "rows/s",
+                    "h2d_bytes_per_step": 128, "d2h_bytes_per_step": res_bytes,
+                    "note": "a step is one request: its descriptor in, its groups back"},
+            "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def serve_cpu_baseline(spec, dims, fact, trace, seconds: float = 10.0):
+    """The oracle's filter + join + group-by on every host thread over the
+    trace's requests against dimensions of at most 3M keys (their rows
+    copied to the host), for about `seconds`: probe rows / s."""
+    import oracle
+    oracle.build()
+    cpu_dims = {}
+    rows = 0
+    t_run = 0.0
+    done = 0
+    for r in trace:
+        if spec.dim_keys[r.dim] > 3_000_000 or r.n_rows > 20_000_000:
+            continue
+        if r.dim not in cpu_dims:
+            cpu_dims[r.dim] = (dims.keys[r.dim].cpu().numpy(), dims.groups[r.dim].cpu().numpy())
+        s = slice(r.row0, r.row0 + r.n_rows)
+        fk, d, v = fact.fk[s].cpu().numpy(), fact.date[s].cpu().numpy(), fact.value[s].cpu().numpy()
+        k, g = cpu_dims[r.dim]
+        a = time.perf_counter()
+        oracle.serve_request(k, g, spec.dim_groups[r.dim], fk, d, v, r.date_lo, r.date_hi)
+        t_run += time.perf_counter() - a
+        rows += r.n_rows
+        done += 1
+        if t_run >= seconds:
+            break
+    if not done:
+        return None
+    return {"value": rows / t_run, "unit": "rows/s", "cores": oracle.threads(), "kind": "port",
+            "sample": f"{done} requests of the trace on dimensions of <= 3M keys, "
+                      f"{rows} probe rows, {t_run:.1f} s"}
+
+
 def main(argv=None) -> int:
     args = parse_args(argv)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -711,6 +891,16 @@ def main(argv=None) -> int:
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.workload == "batch":
         run_batch(args, world, rank, local_rank)
+        return 0
+    if args.workload.startswith("serve"):
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable":
+                                  "the serve workload's reference arm is its plain form per "
+                                  "request, reported as plain_form of --workload serve"}),
+                      flush=True)
+            return 0
+        run_serve(args, world, rank, local_rank)
         return 0
     if args.workload.startswith("paged"):
         if args.impl == "reference":

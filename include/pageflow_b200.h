@@ -328,6 +328,60 @@ int pf_batch_prepare(const pf_batch_instance* instances, int n, void* workspace,
 int pf_batch_run(void* workspace, int64_t* stats, void* stream);
 int64_t* pf_batch_slab(void* workspace, int i);
 
+/* ---- serving: resident dimension tables, requests in persistent launches -- */
+/*
+ * A dimension table's hash table, built once and kept across requests:
+ * 16-byte slots, a power of two of at least 2 x n_keys.  Keys must be unique
+ * (as the reference's unique-hash join requires of its build side); groups
+ * outside [0, n_groups) are kept but never aggregated.  stats (device
+ * int64[2]): rows with a group out of range, rows that found no slot.
+ */
+size_t pf_dim_table_bytes(int64_t n_keys);
+int pf_dim_build(const int64_t* keys, const int32_t* groups, int64_t n_keys, int64_t n_groups,
+                 void* table, size_t table_bytes, int64_t* stats, void* stream);
+/*
+ * One request's share of a launch: SELECT group, SUM(value), COUNT(*) FROM
+ * probe JOIN dim ON probe.fk = dim.key WHERE date_lo <= probe.date < date_hi
+ * GROUP BY dim.group, over the probe rows [row_begin, row_end) of this
+ * launch.  slab: device int64[2 x n_groups] (sum, count) pairs, zero before
+ * the request's first launch, accumulated across its launches.  In the
+ * launch with finish = 1 the occupied groups are written in ascending order
+ * (out_keys / out_sums / out_counts, n_groups rows each; out_n the count)
+ * and the pinned host word *done (may be NULL) is set to 1 + groups once
+ * they are written (all ones if the launch gave up on it).  n_groups <=
+ * 4,194,304.
+ */
+typedef struct {
+  const void* table;
+  int64_t n_keys;
+  int64_t n_groups;
+  const int64_t* fk;
+  const int32_t* date;
+  const int64_t* value;
+  int64_t row_begin, row_end;
+  int32_t date_lo, date_hi;
+  int32_t finish;
+  int32_t pad;
+  int64_t* slab;
+  int64_t* out_keys;
+  int64_t* out_sums;
+  int64_t* out_counts;
+  int64_t* out_n;
+  int64_t* done;
+} pf_serve_request;
+/*
+ * One persistent launch over n requests, in the order given (a request's
+ * items run before the next request's are handed out).  Queued only; the
+ * request list is staged through pinned memory of the calling thread.
+ * stats (device int64[4], zeroed by the caller, added to by every launch):
+ * matched rows, device error word (a bounded wait gave up; the request's
+ * done word is then set to all ones), rows that passed the filter.  No counterpart in the reference:
+ * it serves the serving workload (requests against resident tables).
+ */
+size_t pf_serve_workspace(int max_requests);
+int pf_serve_run(const pf_serve_request* requests, int n, void* workspace,
+                 size_t workspace_bytes, int64_t* stats, void* stream);
+
 /* ---- seeded synthetic inputs (identical to the CPU generator) ------------ */
 /* config ids: 0 = small (250K x 1M, 25 groups), 1 = scale (150M x 600M,
  * 1.5M groups); `rows` and `lo` select rows [lo, lo + rows). */
@@ -341,6 +395,15 @@ int pf_gen_probe(int config, uint64_t seed, int64_t n_build, int64_t lo, int64_t
 int pf_gen_batch_probe(uint64_t seed, int64_t n_build, int64_t lo, int64_t rows, int nbins,
                        const int64_t* edges, const uint64_t* thr, int64_t* fk, int64_t* value,
                        void* stream);
+/* The serving workload: dimension rows [lo, lo + rows) of a dimension of
+ * n_keys keys (the n_keys most referenced of n_ranks ranks), and fact rows
+ * (FK ranks from the Zipf table, dates, values). */
+int pf_gen_serve_dim(uint64_t seed, int64_t n_ranks, uint64_t group_seed, int64_t n_keys,
+                     int64_t n_groups, int64_t lo, int64_t rows, int64_t* key, int32_t* group,
+                     void* stream);
+int pf_gen_serve_fact(uint64_t seed, int64_t n_ranks, int nbins, const int64_t* edges,
+                      const uint64_t* thr, int64_t lo, int64_t rows, int64_t* fk, int32_t* date,
+                      int64_t* value, void* stream);
 
 #ifdef __cplusplus
 }

@@ -71,6 +71,10 @@ def lib():
         L.or_page_decode.restype = _c_i64
         L.or_gen_paged.argtypes = [ctypes.c_uint64, _c_i64, ctypes.c_int, _i64p, _u64p,
                                    _c_i64, _c_i64] + [_i64p] * 6
+        L.or_gen_serve_dim.argtypes = [ctypes.c_uint64, _c_i64, ctypes.c_uint64, _c_i64, _c_i64,
+                                       _c_i64, _i64p, _i32p]
+        L.or_gen_serve_fact.argtypes = [ctypes.c_uint64, _c_i64, ctypes.c_int, _i64p, _u64p,
+                                        _c_i64, _c_i64, _i64p, _i32p, _i64p]
         _lib = L
     return _lib
 
@@ -301,3 +305,38 @@ def paged_scan(cols: dict, n_rows: int, rows_per_page: int, groups_per_batch: in
                 batch[name] = v[r0:r1][keep][order]
         out.append(batch)
     return out
+
+
+# ---- serving workload -----------------------------------------------------
+
+def gen_serve_dim(seed: int, n_ranks: int, group_seed: int, n_groups: int, lo: int, rows: int):
+    """Dimension rows [lo, lo + rows): (keys int64, groups int32)."""
+    k = np.empty(rows, np.int64)
+    g = np.empty(rows, np.int32)
+    lib().or_gen_serve_dim(seed, n_ranks, group_seed, n_groups, lo, rows, k, g)
+    return k, g
+
+
+def gen_serve_fact(seed: int, n_ranks: int, lo: int, rows: int, edges, thr):
+    """Fact rows [lo, lo + rows): (fk int64, date int32, value int64)."""
+    fk = np.empty(rows, np.int64)
+    d = np.empty(rows, np.int32)
+    v = np.empty(rows, np.int64)
+    e = _a(edges)
+    t = np.ascontiguousarray(thr, dtype=np.uint64)
+    lib().or_gen_serve_fact(seed, n_ranks, t.shape[0], e, t, lo, rows, fk, d, v)
+    return fk, d, v
+
+
+def serve_request(dim_keys, dim_groups, n_groups: int, fk, date, value, date_lo: int,
+                  date_hi: int):
+    """One serving request: SELECT group, SUM(value), COUNT(*) FROM fact JOIN
+    dim ON fact.fk = dim.key WHERE date_lo <= date < date_hi GROUP BY
+    dim.group, as (groups ascending, sums, counts) of the occupied groups:
+    the filter (operators/filter.py:10-16), mask compaction
+    (utility/tensor_utils.py:12-39), then or_join_aggregate."""
+    keep = (np.asarray(date) >= date_lo) & (np.asarray(date) < date_hi)
+    s, c, _, _ = join_aggregate(dim_keys, dim_groups, np.asarray(fk)[keep],
+                                np.asarray(value)[keep], None, 1, 0, n_groups, B=16)
+    occ = np.nonzero(c)[0]
+    return occ.astype(np.int64), s[occ], c[occ]

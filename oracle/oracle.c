@@ -552,3 +552,22 @@ void or_gen_paged(uint64_t seed, int64_t n_build, int nbins, const int64_t* edge
     status[i] = (int64_t)pf_range(pf_u(seed, 7, r), 2);
   }
 }
+
+/* The CPU twin of the serving workload's generator (synth.h): dimension rows
+ * [lo, lo + rows) and fact rows [lo, lo + rows). */
+void or_gen_serve_dim(uint64_t seed, int64_t n_ranks, uint64_t group_seed, int64_t n_groups,
+                      int64_t lo, int64_t rows, int64_t* key, int32_t* group) {
+  const pf_perm_t perm = pf_perm_make(seed, (uint64_t)n_ranks);
+  for (int64_t i = 0; i < rows; ++i)
+    pf_gen_serve_dim_row(group_seed, &perm, (uint64_t)n_groups, (uint64_t)(lo + i), &key[i],
+                         &group[i]);
+}
+
+void or_gen_serve_fact(uint64_t seed, int64_t n_ranks, int nbins, const int64_t* edges,
+                       const uint64_t* thr, int64_t lo, int64_t rows, int64_t* fk,
+                       int32_t* date, int64_t* value) {
+  const pf_perm_t perm = pf_perm_make(seed, (uint64_t)n_ranks);
+  for (int64_t i = 0; i < rows; ++i)
+    pf_gen_serve_fact_row(seed, &perm, nbins, edges, thr, (uint64_t)(lo + i), &fk[i], &date[i],
+                          &value[i]);
+}

@@ -76,6 +76,14 @@ _SIGS = {
     "pf_paged_scan_workspace": (_sz, [_vp, _i64, _int, _i64, _int, _int]),
     "pf_paged_scan": (_int, [_vp, _vp, _i64, _int, _vp, _i64, _i64, _int, _int, _i64, _i64,
                              _int, _int, _int, _vp, _i64, _vp, _vp, _vp, _sz, _vp]),
+    "pf_dim_table_bytes": (_sz, [_i64]),
+    "pf_dim_build": (_int, [_vp, _vp, _i64, _i64, _vp, _sz, _vp, _vp]),
+    "pf_serve_workspace": (_sz, [_int]),
+    "pf_serve_run": (_int, [_vp, _int, _vp, _sz, _vp, _vp]),
+    "pf_gen_serve_dim": (_int, [ctypes.c_uint64, _i64, ctypes.c_uint64, _i64, _i64, _i64, _i64,
+                                _vp, _vp, _vp]),
+    "pf_gen_serve_fact": (_int, [ctypes.c_uint64, _i64, _int, _vp, _vp, _i64, _i64, _vp, _vp,
+                                 _vp, _vp]),
     "pf_batch_workspace": (_sz, [_vp, _int]),
     "pf_batch_prepare": (_int, [_vp, _int, _vp, _sz, _vp]),
     "pf_batch_run": (_int, [_vp, _vp, _vp]),
@@ -88,6 +96,16 @@ class BatchInstance(ctypes.Structure):
     _fields_ = [("build_key", _vp), ("build_group", _vp), ("n_build", _i64),
                 ("probe_fk", _vp), ("probe_value", _vp), ("n_probe", _i64),
                 ("group_min", _i64), ("n_groups", _i64)]
+
+class ServeRequest(ctypes.Structure):
+    """pf_serve_request (include/pageflow_b200.h)."""
+    _fields_ = [("table", _vp), ("n_keys", _i64), ("n_groups", _i64), ("fk", _vp),
+                ("date", _vp), ("value", _vp), ("row_begin", _i64), ("row_end", _i64),
+                ("date_lo", ctypes.c_int32), ("date_hi", ctypes.c_int32),
+                ("finish", ctypes.c_int32), ("pad", ctypes.c_int32), ("slab", _vp),
+                ("out_keys", _vp), ("out_sums", _vp), ("out_counts", _vp), ("out_n", _vp),
+                ("done", _vp)]
+
 
 _lib = None
 

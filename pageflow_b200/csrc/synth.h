@@ -19,6 +19,13 @@
  *                 fk = (miss ? N + 1 : 1) + range(u(seed,3,r), N)
  *                 price = 90000 + range(u(seed,4,r), 10410001)    cents
  *                 disc  = range(u(seed,5,r), 11)                  hundredths
+ *
+ * Serving workload (N ranked keys; a dimension of n keys holds the n most
+ * referenced ranks, so smaller dimensions hold hotter keys):
+ *   dimension row r:  key = 1 + perm(seed, N)(r), group = range(u(gseed,1,r), G)
+ *   fact row r:       fk = 1 + perm(seed, N)(zipf rank(u(seed,2,r), u(seed,3,r)))
+ *                     date = 8035 + range(u(seed,4,r), 2557)         days
+ *                     value = 90000 + range(u(seed,5,r), 10410001)   cents
  */
 #ifndef PF_SYNTH_H
 #define PF_SYNTH_H
@@ -154,6 +161,21 @@ PF_HD void pf_gen_batch_probe_row(uint64_t seed, const pf_perm_t* perm, int nbin
   const uint64_t rank = pf_zipf_rank(pf_u(seed, 3, r), pf_u(seed, 4, r), nbins, edges, thr);
   *fk = (int64_t)(1 + pf_perm(perm, rank));
   *value = (int64_t)pf_range(pf_u(seed, 5, r), 10000000);
+}
+
+PF_HD void pf_gen_serve_dim_row(uint64_t gseed, const pf_perm_t* perm, uint64_t n_groups,
+                                uint64_t r, int64_t* key, int32_t* group) {
+  *key = (int64_t)(1 + pf_perm(perm, r));
+  *group = (int32_t)pf_range(pf_u(gseed, 1, r), n_groups);
+}
+
+PF_HD void pf_gen_serve_fact_row(uint64_t seed, const pf_perm_t* perm, int nbins,
+                                 const int64_t* edges, const uint64_t* thr, uint64_t r,
+                                 int64_t* fk, int32_t* date, int64_t* value) {
+  const uint64_t rank = pf_zipf_rank(pf_u(seed, 2, r), pf_u(seed, 3, r), nbins, edges, thr);
+  *fk = (int64_t)(1 + pf_perm(perm, rank));
+  *date = (int32_t)(8035 + pf_range(pf_u(seed, 4, r), 2557));
+  *value = (int64_t)(90000 + pf_range(pf_u(seed, 5, r), 10410001));
 }
 
 #endif /* PF_SYNTH_H */
