@@ -88,6 +88,36 @@ def measured_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
+# ---- replicas ----------------------------------------------------------------------
+
+def max_over_ranks(ms: float, world: int, device) -> float:
+    """The job's time: the slowest rank's (every rank runs its own replica)."""
+    if world == 1:
+        return float(ms)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x: float, world: int, device) -> float:
+    """The sum of a per-rank quantity over the ranks."""
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def job_rate(units_per_rank: float, ms: float, world: int) -> float:
+    """Whole-job throughput: the units all ranks processed over the job's
+    time (weak scaling: each rank processes units_per_rank)."""
+    return world * units_per_rank / (ms / 1e3)
+
+
 # ---- clocks -------------------------------------------------------------------
 
 class ClockSampler:
@@ -281,13 +311,9 @@ def run_ours(args, w, world, rank, local_rank):
     if world > 1:
         dist.barrier()
     clocks = sampler.stop()
-    ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), world, dev)
     rows_step = w.n_build + w.n_probe
-    value = world * rows_step * args.steps / (ms / 1e3)
+    value = job_rate(rows_step * args.steps, ms, world)
 
     # roofline: the dominant kernel's live figure and the whole step's
     peak, peak_kind = measured_peak()
@@ -423,12 +449,8 @@ def run_e2e(args, w, plan, dev, dev_inputs, world):
         _, d2h = step()
     e1.record(stream)
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item())
-    value = world * (w.n_build + w.n_probe) * args.e2e_steps / (ms / 1e3)
+    ms = max_over_ranks(e0.elapsed_time(e1), world, dev)
+    value = job_rate((w.n_build + w.n_probe) * args.e2e_steps, ms, world)
     return {"value": value, "unit": "rows/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": ms / args.e2e_steps,
             "h2d_gbs": h2d / (ms / args.e2e_steps / 1e3) / 1e9}
@@ -474,7 +496,8 @@ def run_batch(args, world, rank, local_rank):
         g.replay()
     e1.record()
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
+    ms = max_over_ranks(e0.elapsed_time(e1), world, dev) / args.steps
+    all_rows = sum_over_ranks(rows, world, dev)
     st = b.read_stats()
     # the same instances, one fused-path launch sequence each
     plans = [JoinAggregate(x.build_key.numel(), x.probe_fk.numel(), 0, x.n_groups, dev,
@@ -511,7 +534,7 @@ def run_batch(args, world, rank, local_rank):
                  "ms": pms}
     if rank == 0:
         line = {
-            "metric": "join+agg rows/s (batched)", "value": world * rows / (ms / 1e3),
+            "metric": "join+agg rows/s (batched)", "value": all_rows / (ms / 1e3),
             "unit": "rows/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded, on device)",
@@ -612,7 +635,7 @@ def run_paged(args, world, rank, local_rank):
     prof = _native.profile_end()
     launches = _native.launch_count() - launches0
     clocks = sampler.stop()
-    ms = e0.elapsed_time(e1) / args.steps
+    ms = max_over_ranks(e0.elapsed_time(e1), world, dev) / args.steps
 
     # end to end: the same pass plus the bucket offsets and counters read back
     e0.record(stream)
@@ -622,7 +645,7 @@ def run_paged(args, world, rank, local_rank):
         st_h = p.stats.to("cpu", non_blocking=True)
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world, dev) / args.e2e_steps
     d2h = offs_h.numel() * 8 + st_h.numel() * 8
 
     peak, peak_kind = measured_peak()
@@ -833,7 +856,7 @@ def run_serve(args, world, rank, local_rank):
     if rank == 0:
         line = {
             "metric": "serving rows/s at the highest offered rate; p50/p99 latency per rate",
-            "value": world * top["rows_per_s"], "unit": "rows/s", "n_gpus": world,
+            "value": job_rows_per_s, "unit": "rows/s", "n_gpus": world,
             "steps": n, "warmup": args.warmup, "ms_per_step": 1e3 / top["completed_per_s"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "int64", "data": "synthetic (seeded generator, resident on the device)",
@@ -844,7 +867,7 @@ def run_serve(args, world, rank, local_rank):
                        "setup_s": setup_s,
                        "l2": "requests scan slices of a 20 GB fact pool, far above L2"},
             "sweep": sweep, "knee_rate": knee, "plain_form": plain,
-            "e2e": {"value": world * top["rows_per_s"], "unit": "rows/s",
+            "e2e": {"value": job_rows_per_s, "unit": "rows/s",
                     "h2d_bytes_per_step": 128, "d2h_bytes_per_step": res_bytes,
                     "note": "a step is one request: its descriptor in, its groups back"},
             "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
@@ -889,32 +912,23 @@ def main(argv=None) -> int:
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.workload == "batch":
-        run_batch(args, world, rank, local_rank)
-        return 0
-    if args.workload.startswith("serve"):
-        if args.impl == "reference":
-            if rank == 0:
-                print(json.dumps({"impl": "reference", "unavailable":
-                                  "the serve workload's reference arm is its plain form per "
-                                  "request, reported as plain_form of --workload serve"}),
-                      flush=True)
-            return 0
-        run_serve(args, world, rank, local_rank)
-        return 0
-    if args.workload.startswith("paged"):
-        if args.impl == "reference":
-            if rank == 0:
-                print(json.dumps({"impl": "reference", "unavailable":
-                                  "the paged workload's reference arm is the oracle decoder, "
-                                  "reported as cpu_baseline of --workload paged"}), flush=True)
-            return 0
-        run_paged(args, world, rank, local_rank)
-        return 0
-    w = workload(args.workload)
+    mode = args.workload.split("/", 1)[0]
     if args.impl == "reference":
-        run_reference(args, w, world, rank)
+        if mode in ("serve", "paged", "batch"):
+            if rank == 0:
+                why = {"serve": "the serve workload's reference arm is its plain form per "
+                                "request, reported as plain_form of --workload serve",
+                       "paged": "the paged workload's reference arm is the oracle decoder, "
+                                "reported as cpu_baseline of --workload paged",
+                       "batch": "the batch workload's reference arm is the plain form per "
+                                "instance, reported as plain_form_per_instance of --workload "
+                                "batch"}[mode]
+                print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
+            return 0
+        run_reference(args, workload(args.workload), world, rank)
         return 0
+    run = {"batch": run_batch, "serve": run_serve, "paged": run_paged}.get(mode)
+    w = None if run else workload(args.workload)
     if world > 1:
         import datetime
 
@@ -924,7 +938,10 @@ def main(argv=None) -> int:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
     try:
-        run_ours(args, w, world, rank, local_rank)
+        if run:
+            run(args, world, rank, local_rank)
+        else:
+            run_ours(args, w, world, rank, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist
