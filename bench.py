@@ -516,7 +516,7 @@ def run_batch(args, world, rank, local_rank):
     ms_pi = e0.elapsed_time(e1)
     plain = None
     from oracle import plain_form
-    if plain_form.available():
+    if plain_form.available() and not args.no_plain_form:
         k = min(len(insts), args.plain_instances or len(insts))
         sub_rows = sum(insts[i].build_key.numel() + insts[i].probe_fk.numel() for i in range(k))
         def plain_run():
@@ -841,6 +841,7 @@ def run_serve(args, world, rank, local_rank):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = serve_cpu_baseline(spec, dims, fact, trace)
     top = sweep[-1]
+    job_rows_per_s = sum_over_ranks(top["rows_per_s"], world, dev)
     # the knee: the highest rate still served as offered (completions keep up
     # with the trace's realised arrival rate) with p99 within 10x of the
     # lowest rate's

@@ -181,3 +181,39 @@ def test_static_scratch_join_refuses_sizes_before_any_device_work():
         assert b"static scratch" in L.pf_last_error()
     rc = L.pf_join_unique_hash_static(fake, None, 10, fake, None, 10, 3, fake, fake, fake, None)
     assert rc == _native.PF_EINVAL
+
+
+def test_bench_functions_name_only_defined_names():
+    # every name a bench.py function loads is a local, a module-level name or
+    # a builtin: the GPU-only paths cannot fail on a misspelt name at run time
+    import ast
+    import builtins
+    tree = ast.parse((REPO / "bench.py").read_text())
+    top = set()
+    for n in tree.body:
+        if isinstance(n, (ast.FunctionDef, ast.ClassDef)):
+            top.add(n.name)
+        elif isinstance(n, ast.Assign):
+            top |= {t.id for t in n.targets if isinstance(t, ast.Name)}
+        elif isinstance(n, (ast.Import, ast.ImportFrom)):
+            top |= {a.asname or a.name.split(".")[0] for a in n.names}
+    missing = []
+    for fn in (n for n in tree.body if isinstance(n, ast.FunctionDef)):
+        local = {a.arg for a in fn.args.args + fn.args.kwonlyargs}
+        for node in ast.walk(fn):
+            if isinstance(node, ast.Name) and isinstance(node.ctx, ast.Store):
+                local.add(node.id)
+            elif isinstance(node, (ast.Import, ast.ImportFrom)):
+                local |= {a.asname or a.name.split(".")[0] for a in node.names}
+            elif isinstance(node, (ast.FunctionDef, ast.Lambda)) and node is not fn:
+                local |= {a.arg for a in node.args.args}
+                if isinstance(node, ast.FunctionDef):
+                    local.add(node.name)
+            elif isinstance(node, ast.ExceptHandler) and node.name:
+                local.add(node.name)
+        for node in ast.walk(fn):
+            if (isinstance(node, ast.Name) and isinstance(node.ctx, ast.Load)
+                    and node.id not in local and node.id not in top
+                    and not hasattr(builtins, node.id)):
+                missing.append(f"{fn.name}:{node.lineno}:{node.id}")
+    assert missing == []
