@@ -370,8 +370,8 @@ typedef struct {
   int64_t* done;
 } pf_serve_request;
 /*
- * One persistent launch over n requests, in the order given (a request's
- * items run before the next request's are handed out).  Queued only; the
+ * One persistent launch over n requests (1 <= n <= 8192), in the order given
+ * (a request's items run before the next request's are handed out).  Queued only; the
  * request list is staged through pinned memory of the calling thread.
  * stats (device int64[4], zeroed by the caller, added to by every launch):
  * matched rows, device error word (a bounded wait gave up; the request's

@@ -28,6 +28,10 @@ namespace pf {
 namespace {
 
 constexpr int BT2 = 256;
+#ifndef PF_BATCH_BV
+#define PF_BATCH_BV 1
+#endif
+constexpr int BV = PF_BATCH_BV;  // rows a thread keeps in flight
 constexpr int BITEM = 4096;
 constexpr int PITEM = 8192;
 constexpr unsigned WAIT_LIMIT = 1u << 24;  // polls of a probe item's wait (x ~0.5 us)
@@ -66,18 +70,20 @@ struct Layout {
   Header* header;
   Desc* desc;
   unsigned* remaining;
+  int* imap;  // work item -> instance
   Slot* tables;
   unsigned long long* slabs;
   unsigned long long table_slots, slab_pairs;
 };
 
 Layout layout(char* base, int n, unsigned long long table_slots, unsigned long long slab_pairs,
-              size_t* used) {
+              unsigned long long items, size_t* used) {
   Arena a(base, ~(size_t)0);
   Layout l{};
   l.header = a.take<Header>(1);
   l.desc = a.take<Desc>(std::max(n, 1));
   l.remaining = a.take<unsigned>(std::max(n, 1));
+  l.imap = a.take<int>(std::max<unsigned long long>(items, 1));
   l.tables = a.take<Slot>(std::max<unsigned long long>(table_slots, 1));
   l.slabs = a.take<unsigned long long>(2 * std::max<unsigned long long>(slab_pairs, 1));
   l.table_slots = table_slots;
@@ -86,12 +92,17 @@ Layout layout(char* base, int n, unsigned long long table_slots, unsigned long l
   return l;
 }
 
-void totals(const pf_batch_instance* in, int n, unsigned long long* ts, unsigned long long* sp) {
+void totals(const pf_batch_instance* in, int n, unsigned long long* ts, unsigned long long* sp,
+            unsigned long long* items) {
   *ts = 0;
   *sp = 0;
+  *items = 0;
   for (int i = 0; i < n; ++i) {
-    *ts += 2ULL * (unsigned long long)std::max<int64_t>(in[i].n_build, 0);
+    const long long nb = std::max<int64_t>(in[i].n_build, 0);
+    const long long np = nb > 0 ? std::max<int64_t>(in[i].n_probe, 0) : 0;
+    *ts += 2ULL * (unsigned long long)nb;
     *sp += (unsigned long long)std::max<int64_t>(in[i].n_groups, 0);
+    *items += (unsigned long long)((nb + BITEM - 1) / BITEM + (np + PITEM - 1) / PITEM);
   }
 }
 
@@ -110,62 +121,83 @@ __global__ void k_batch_reset(Header* h, Desc* d, unsigned* remaining, int n,
   for (long long i = tid; i < (long long)words; i += stride) slabs[i] = 0;
 }
 
-// The instance of item `it`: the last instance whose first item is <= it.
-__device__ __forceinline__ int instance_of(const Desc* d, int n, long long it) {
-  int lo = 0, hi = n - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (d[mid].item0 <= it) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
-}
-
 __device__ __forceinline__ unsigned first_slot(uint64_t h, unsigned long long cap) {
   return (unsigned)(((h >> 32) * cap) >> 32);
 }
 
-__global__ void __launch_bounds__(BT2) k_batch(Header* h, const Desc* d, unsigned* remaining,
+__global__ void __launch_bounds__(BT2) k_batch(Header* h, const Desc* d, const int* __restrict__ imap,
+                                               unsigned* remaining,
                                                Slot* tables, unsigned long long* slabs,
                                                unsigned long long* stats) {
   __shared__ long long item_s;
   __shared__ int ok_s;
   const unsigned epoch = h->epoch;
   const long long ni = h->n_items;
-  const int n = h->n_inst;
   unsigned long long matched = 0, bad_group = 0, overflow = 0;
+  // With PF_PREFETCH_ITEMS, thread 0 takes the block's next item while the
+  // block works on the current one (measured no faster, so off by default).
+  // Items are taken in increasing order and an item waits only for items
+  // before it, so the smallest unfinished item is always some block's
+  // current item with nothing left to wait for: the launch progresses.
+  if (threadIdx.x == 0) item_s = (long long)atomicAdd(&h->counter, 1ULL);
   while (true) {
-    __syncthreads();
-    if (threadIdx.x == 0) item_s = (long long)atomicAdd(&h->counter, 1ULL);
     __syncthreads();
     const long long it = item_s;
     if (it >= ni) break;
-    const int inst = instance_of(d, n, it);
+    unsigned long long next = 0;
+    if (PF_PREFETCH_ITEMS && threadIdx.x == 0) next = atomicAdd(&h->counter, 1ULL);
+    const int inst = imap[it];
     const Desc& D = d[inst];
     const long long local = it - D.item0;
     if (local < D.nbi) {
+      // BV rows a thread at a time: loads, then every first claim, then the
+      // (rare) collisions
       const long long lo = local * BITEM, hi = min(D.nb, lo + BITEM);
-      for (long long i = lo + threadIdx.x; i < hi; i += BT2) {
-        const unsigned long long key = (unsigned long long)D.bkey[i];
-        const long long g = (long long)D.bgrp[i] - D.gmin;
-        uint32_t goff = 0xffffffffu;
-        if (g >= 0 && g < D.ng) goff = (uint32_t)g;
-        else ++bad_group;
-        const uint64_t hh = mix64(key);
-        unsigned pos = first_slot(hh, D.tcap);
-        bool done = false;
-        for (unsigned long long left = D.tcap; left > 0; --left) {
-          Slot* sl = tables + D.toff + pos;
+      for (long long i0 = lo; i0 < hi; i0 += BT2 * BV) {
+        unsigned long long key[BV];
+        uint32_t goff[BV];
+        unsigned pos[BV];
+        bool live[BV], done[BV];
+#pragma unroll
+        for (int k = 0; k < BV; ++k) {
+          const long long i = i0 + k * BT2 + threadIdx.x;
+          live[k] = i < hi;
+          key[k] = live[k] ? (unsigned long long)D.bkey[i] : 0ULL;
+          const long long g = live[k] ? (long long)D.bgrp[i] - D.gmin : 0;
+          goff[k] = 0xffffffffu;
+          if (g >= 0 && g < D.ng) goff[k] = (uint32_t)g;
+          else if (live[k]) ++bad_group;
+        }
+#pragma unroll
+        for (int k = 0; k < BV; ++k) {
+          pos[k] = first_slot(mix64(key[k]), D.tcap);
+          done[k] = false;
+          if (!live[k]) continue;
+          Slot* sl = tables + D.toff + pos[k];
           unsigned* tag = reinterpret_cast<unsigned*>(&sl->tagged) + 1;
           if (atomicMax(tag, epoch) < epoch) {
             *reinterpret_cast<ulonglong2*>(sl) =
-                make_ulonglong2(key, ((unsigned long long)epoch << 32) | goff);
-            done = true;
-            break;
+                make_ulonglong2(key[k], ((unsigned long long)epoch << 32) | goff[k]);
+            done[k] = true;
           }
-          if (++pos == D.tcap) pos = 0;
         }
-        overflow += !done;
+#pragma unroll
+        for (int k = 0; k < BV; ++k) {
+          if (!live[k] || done[k]) continue;
+          unsigned p = pos[k];
+          for (unsigned long long left = D.tcap - 1; left > 0; --left) {
+            if (++p == D.tcap) p = 0;
+            Slot* sl = tables + D.toff + p;
+            unsigned* tag = reinterpret_cast<unsigned*>(&sl->tagged) + 1;
+            if (atomicMax(tag, epoch) < epoch) {
+              *reinterpret_cast<ulonglong2*>(sl) =
+                  make_ulonglong2(key[k], ((unsigned long long)epoch << 32) | goff[k]);
+              done[k] = true;
+              break;
+            }
+          }
+          overflow += !done[k];
+        }
       }
       __syncthreads();
       if (threadIdx.x == 0) {
@@ -184,33 +216,57 @@ __global__ void __launch_bounds__(BT2) k_batch(Header* h, const Desc* d, unsigne
         __threadfence();
       }
       __syncthreads();
-      if (!ok_s) continue;
+      if (!ok_s) {
+        if (threadIdx.x == 0) item_s = (long long)(PF_PREFETCH_ITEMS ? next : atomicAdd(&h->counter, 1ULL));
+        continue;
+      }
+      // BV rows a thread at a time: keys, then every first slot and value,
+      // then the (rare) collisions
       const long long lo = (local - D.nbi) * PITEM, hi = min(D.np, lo + PITEM);
-      for (long long i0 = lo; i0 < hi; i0 += BT2) {
-        const long long i = i0 + threadIdx.x;
-        long long g = -1, value = 0;
-        if (i < hi && D.tcap > 0) {
-          const unsigned long long key = (unsigned long long)D.pfk[i];
-          const uint64_t hh = mix64(key);
-          unsigned pos = first_slot(hh, D.tcap);
+      for (long long i0 = lo; i0 < hi; i0 += BT2 * BV) {
+        unsigned long long key[BV];
+        unsigned pos[BV];
+        ulonglong2 sl[BV];
+        long long value[BV], g[BV];
+        bool live[BV];
+#pragma unroll
+        for (int k = 0; k < BV; ++k) {
+          const long long i = i0 + k * BT2 + threadIdx.x;
+          live[k] = i < hi && D.tcap > 0;
+          key[k] = live[k] ? (unsigned long long)D.pfk[i] : 0ULL;
+        }
+#pragma unroll
+        for (int k = 0; k < BV; ++k) {
+          const long long i = i0 + k * BT2 + threadIdx.x;
+          pos[k] = live[k] ? first_slot(mix64(key[k]), D.tcap) : 0u;
+          sl[k] = live[k] ? __ldcg(reinterpret_cast<const ulonglong2*>(tables + D.toff + pos[k]))
+                          : make_ulonglong2(0ULL, 0ULL);
+          value[k] = live[k] ? D.pval[i] : 0;
+        }
+#pragma unroll
+        for (int k = 0; k < BV; ++k) {
+          g[k] = -1;
+          if (!live[k]) continue;
+          ulonglong2 x = sl[k];
+          unsigned p = pos[k];
           for (unsigned long long probes = 0; probes < D.tcap; ++probes) {
-            const ulonglong2 sl = __ldcg(reinterpret_cast<const ulonglong2*>(tables + D.toff + pos));
-            if ((uint32_t)(sl.y >> 32) != epoch) break;
-            if (sl.x == key) {
+            if ((uint32_t)(x.y >> 32) != epoch) break;
+            if (x.x == key[k]) {
               ++matched;
-              const uint32_t go = (uint32_t)sl.y;
-              if (go != 0xffffffffu) {
-                g = go;
-                value = D.pval[i];
-              }
+              const uint32_t go = (uint32_t)x.y;
+              if (go != 0xffffffffu) g[k] = go;
               break;
             }
-            if (++pos == D.tcap) pos = 0;
+            if (++p == D.tcap) p = 0;
+            x = __ldcg(reinterpret_cast<const ulonglong2*>(tables + D.toff + p));
           }
         }
-        combined_add(slabs + 2 * D.soff, g, value);
+#pragma unroll
+        for (int k = 0; k < BV; ++k) combined_add(slabs + 2 * D.soff, g[k], g[k] >= 0 ? value[k] : 0);
       }
     }
+    __syncthreads();  // every thread has read item_s
+    if (threadIdx.x == 0) item_s = (long long)(PF_PREFETCH_ITEMS ? next : atomicAdd(&h->counter, 1ULL));
   }
   for (int o = 16; o; o >>= 1) matched += __shfl_xor_sync(FULL, matched, o);
   if ((threadIdx.x & 31) == 0 && matched) atomicAdd(&stats[0], matched);
@@ -227,7 +283,7 @@ __global__ void k_batch_error(const Header* h, unsigned long long* stats) {
 // copy of device memory and can be captured.
 struct HostPlan {
   int n = 0;
-  unsigned long long table_slots = 0, slab_pairs = 0;
+  unsigned long long table_slots = 0, slab_pairs = 0, items = 0;
   std::vector<unsigned long long> slab_off;
 };
 
@@ -256,10 +312,10 @@ int batch_grid(int* grid) {
 using namespace pf;
 
 extern "C" size_t pf_batch_workspace(const pf_batch_instance* in, int n) {
-  unsigned long long ts, sp;
-  totals(in, n, &ts, &sp);
+  unsigned long long ts, sp, items;
+  totals(in, n, &ts, &sp, &items);
   size_t used = 0;
-  layout(nullptr, n, ts, sp, &used);
+  layout(nullptr, n, ts, sp, items, &used);
   return used + 256;
 }
 
@@ -267,10 +323,10 @@ extern "C" int pf_batch_prepare(const pf_batch_instance* in, int n, void* worksp
                                 size_t workspace_bytes, void* stream) {
   cudaStream_t st = (cudaStream_t)stream;
   if (n < 1) return fail(PF_EINVAL, "batch: at least one instance");
-  unsigned long long ts, sp;
-  totals(in, n, &ts, &sp);
+  unsigned long long ts, sp, items;
+  totals(in, n, &ts, &sp, &items);
   size_t used = 0;
-  Layout l = layout((char*)workspace, n, ts, sp, &used);
+  Layout l = layout((char*)workspace, n, ts, sp, items, &used);
   if (!workspace || used > workspace_bytes)
     return fail(PF_ENOSPACE, "batch: workspace of %zu bytes, %zu needed", workspace_bytes, used);
   std::vector<Desc> d(n);
@@ -310,6 +366,15 @@ extern "C" int pf_batch_prepare(const pf_batch_instance* in, int n, void* worksp
   hh.n_build_items = bi;
   hh.n_items = bi + pi;
   hh.n_inst = n;
+  if ((unsigned long long)(bi + pi) != items)
+    return fail(PF_EINVAL, "batch: %lld work items, %llu planned", bi + pi, items);
+  std::vector<int> imap((size_t)std::max<unsigned long long>(items, 1), 0);
+  for (int i = 0; i < n; ++i) {
+    const long long nit = d[i].nbi + (d[i].np + PITEM - 1) / PITEM;
+    for (long long k = 0; k < nit; ++k) imap[(size_t)(d[i].item0 + k)] = i;
+  }
+  PF_CUDA(cudaMemcpyAsync(l.imap, imap.data(), sizeof(int) * imap.size(), cudaMemcpyHostToDevice,
+                          st));
   PF_CUDA(cudaMemcpyAsync(l.desc, d.data(), sizeof(Desc) * n, cudaMemcpyHostToDevice, st));
   PF_CUDA(cudaMemcpyAsync(l.header, &hh, sizeof(Header), cudaMemcpyHostToDevice, st));
   PF_CUDA(cudaMemsetAsync(l.tables, 0, sizeof(Slot) * std::max<unsigned long long>(ts, 1), st));
@@ -318,6 +383,7 @@ extern "C" int pf_batch_prepare(const pf_batch_instance* in, int n, void* worksp
   hp.n = n;
   hp.table_slots = ts;
   hp.slab_pairs = sp;
+  hp.items = items;
   hp.slab_off.resize(n);
   for (int i = 0; i < n; ++i) hp.slab_off[i] = d[i].soff;
   {
@@ -332,7 +398,7 @@ extern "C" int pf_batch_run(void* workspace, int64_t* stats, void* stream) {
   HostPlan hp;
   if (!find_plan(workspace, &hp)) return fail(PF_EINVAL, "batch: workspace was not prepared");
   if (!stats) return fail(PF_EINVAL, "batch: null stats");
-  Layout l = layout((char*)workspace, hp.n, hp.table_slots, hp.slab_pairs, nullptr);
+  Layout l = layout((char*)workspace, hp.n, hp.table_slots, hp.slab_pairs, hp.items, nullptr);
   int grid = 0;
   if (int rc = batch_grid(&grid)) return rc;
   PF_CUDA(cudaMemsetAsync(stats, 0, 4 * sizeof(int64_t), st));
@@ -347,7 +413,7 @@ extern "C" int pf_batch_run(void* workspace, int64_t* stats, void* stream) {
   PF_LAUNCH("k_batch_reset");
   {
     PF_KERNEL("k_batch", st);
-    k_batch<<<grid, BT2, 0, st>>>(l.header, l.desc, l.remaining, l.tables, l.slabs,
+    k_batch<<<grid, BT2, 0, st>>>(l.header, l.desc, l.imap, l.remaining, l.tables, l.slabs,
                                   (unsigned long long*)stats);
   }
   PF_LAUNCH("k_batch");
@@ -362,6 +428,6 @@ extern "C" int pf_batch_run(void* workspace, int64_t* stats, void* stream) {
 extern "C" int64_t* pf_batch_slab(void* workspace, int i) {
   HostPlan hp;
   if (!find_plan(workspace, &hp) || i < 0 || i >= hp.n) return nullptr;
-  Layout l = layout((char*)workspace, hp.n, hp.table_slots, hp.slab_pairs, nullptr);
+  Layout l = layout((char*)workspace, hp.n, hp.table_slots, hp.slab_pairs, hp.items, nullptr);
   return (int64_t*)(l.slabs + 2 * hp.slab_off[i]);
 }

@@ -24,6 +24,7 @@
 // blocks that are running, so every wait ends.  The host sees a request
 // complete through its done word while the launch goes on with others.
 #include <algorithm>
+#include <climits>
 #include <cstring>
 #include <map>
 
@@ -33,10 +34,15 @@ namespace pf {
 namespace {
 
 constexpr int ST = 256;
+#ifndef PF_SERVE_SV
+#define PF_SERVE_SV 2
+#endif
+constexpr int SV = PF_SERVE_SV;  // probe rows a thread keeps in flight
 constexpr long long PROBE_ROWS = 16384;
 constexpr long long GROUP_CHUNK = 16384;
 constexpr long long MAX_CHUNKS = 256;  // groups <= 4M a request
 constexpr unsigned WAIT_LIMIT = 1u << 22;
+constexpr int MAX_REQUESTS = 8192;  // a launch's requests (their first items sit in smem)
 constexpr unsigned long long OCCUPIED = 1ULL << 63;
 constexpr unsigned long long NO_GROUP = 0xffffffffULL;
 
@@ -112,12 +118,13 @@ struct SHead {
   unsigned long long error;
 };
 
-// The request of item `it`: the last request whose first item is <= it.
-__device__ __forceinline__ int request_of(const SReq* r, int n, long long it) {
+// The request of item `it`: the last request whose first item is <= it
+// (first[] holds every request's first item, in shared memory).
+__device__ __forceinline__ int request_of(const int* first, int n, long long it) {
   int lo = 0, hi = n - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
-    if (r[mid].item0 <= it) lo = mid;
+    if (first[mid] <= it) lo = mid;
     else hi = mid - 1;
   }
   return lo;
@@ -157,52 +164,85 @@ __device__ __forceinline__ long long block_sum(long long v, long long* red) {
 __global__ void __launch_bounds__(ST) k_serve(SHead* h, const SReq* __restrict__ reqs,
                                               SCounters* cnt, long long* chunk_counts,
                                               unsigned long long* stats) {
+  extern __shared__ int first_item[];
   __shared__ long long item_s;
   __shared__ int ok_s;
   __shared__ long long red[ST / 32];
   __shared__ int wpre[ST / 32];
   const long long ni = h->n_items;
   const int n = h->n_req;
+  for (int i = threadIdx.x; i < n; i += ST) first_item[i] = (int)reqs[i].item0;
   unsigned long long matched = 0, kept = 0;
+  Combiner comb;
+  // With PF_PREFETCH_ITEMS, thread 0 takes the block's next item while the
+  // block works on the current one (measured no faster, so off by default).
+  // Items are taken in increasing order and an item waits only for items
+  // before it, so the smallest unfinished item is always some block's
+  // current item with nothing left to wait for: the launch progresses.
+  if (threadIdx.x == 0) item_s = (long long)atomicAdd(&h->counter, 1ULL);
   while (true) {
-    __syncthreads();
-    if (threadIdx.x == 0) item_s = (long long)atomicAdd(&h->counter, 1ULL);
     __syncthreads();
     const long long it = item_s;
     if (it >= ni) break;
-    const int q = request_of(reqs, n, it);
+    unsigned long long next = 0;
+    if (PF_PREFETCH_ITEMS && threadIdx.x == 0) next = atomicAdd(&h->counter, 1ULL);
+    const int q = request_of(first_item, n, it);
     const SReq& R = reqs[q];
     const long long local = it - R.item0;
     if (local < R.npi) {
-      // ---- probe rows
+      // ---- probe rows, SV a thread at a time: every stage (dates, keys, first
+      // slots, values) is issued for all SV rows before any is used, so a
+      // thread keeps SV independent loads in flight
       const long long lo = R.r0 + local * PROBE_ROWS, hi = min(R.r1, lo + PROBE_ROWS);
       const unsigned long long mask = (1ULL << R.logcap) - 1;
-      for (long long i0 = lo; i0 < hi; i0 += ST) {
-        const long long i = i0 + threadIdx.x;
-        long long g = -1, value = 0;
-        if (i < hi) {
-          const int d = R.date[i];
-          if (d >= R.lo && d < R.hi) {
-            ++kept;
-            const unsigned long long key = (unsigned long long)R.fk[i];
-            unsigned long long s = dim_first_slot(mix64(key), R.logcap);
-            for (unsigned long long probes = 0; probes <= mask; ++probes) {
-              const ulonglong2 sl = *reinterpret_cast<const ulonglong2*>(R.table + s);
-              if (sl.y == 0) break;
-              if (sl.x == key) {
-                ++matched;
-                const unsigned long long go = sl.y & ~OCCUPIED;
-                if (go != NO_GROUP) {
-                  g = (long long)go;
-                  value = R.value[i];
-                }
-                break;
-              }
-              s = (s + 1) & mask;
+      for (long long i0 = lo; i0 < hi; i0 += ST * SV) {
+        bool keep[SV];
+        unsigned long long key[SV], slot[SV];
+        ulonglong2 sl[SV];
+        long long g[SV], value[SV];
+#pragma unroll
+        for (int k = 0; k < SV; ++k) {
+          const long long i = i0 + k * ST + threadIdx.x;
+          const int d = i < hi ? R.date[i] : INT_MIN;
+          keep[k] = d >= R.lo && d < R.hi;
+        }
+#pragma unroll
+        for (int k = 0; k < SV; ++k) {
+          const long long i = i0 + k * ST + threadIdx.x;
+          key[k] = keep[k] ? (unsigned long long)R.fk[i] : 0ULL;
+        }
+#pragma unroll
+        for (int k = 0; k < SV; ++k) {
+          slot[k] = dim_first_slot(mix64(key[k]), R.logcap);
+          sl[k] = keep[k] ? *reinterpret_cast<const ulonglong2*>(R.table + slot[k])
+                          : make_ulonglong2(0ULL, 0ULL);
+        }
+#pragma unroll
+        for (int k = 0; k < SV; ++k) {
+          g[k] = -1;
+          if (!keep[k]) continue;
+          ++kept;
+          unsigned long long sk = slot[k];
+          ulonglong2 x = sl[k];
+          for (unsigned long long probes = 0; probes <= mask; ++probes) {
+            if (x.y == 0) break;
+            if (x.x == key[k]) {
+              ++matched;
+              const unsigned long long go = x.y & ~OCCUPIED;
+              if (go != NO_GROUP) g[k] = (long long)go;
+              break;
             }
+            sk = (sk + 1) & mask;
+            x = *reinterpret_cast<const ulonglong2*>(R.table + sk);
           }
         }
-        combined_add(R.slab, g, value);
+#pragma unroll
+        for (int k = 0; k < SV; ++k) {
+          const long long i = i0 + k * ST + threadIdx.x;
+          value[k] = g[k] >= 0 ? R.value[i] : 0;
+        }
+#pragma unroll
+        for (int k = 0; k < SV; ++k) adaptive_add(R.slab, g[k], value[k], comb);
       }
       __syncthreads();
       if (threadIdx.x == 0) {
@@ -214,7 +254,10 @@ __global__ void __launch_bounds__(ST) k_serve(SHead* h, const SReq* __restrict__
       const long long c = local - R.npi;
       if (threadIdx.x == 0) ok_s = wait_zero(&cnt[q].probe_left, h, R.done);
       __syncthreads();
-      if (!ok_s) continue;
+      if (!ok_s) {
+        if (threadIdx.x == 0) item_s = (long long)(PF_PREFETCH_ITEMS ? next : atomicAdd(&h->counter, 1ULL));
+        continue;
+      }
       const long long g0 = c * GROUP_CHUNK, g1 = min(R.ng, g0 + GROUP_CHUNK);
       long long occ = 0;
       for (long long g = g0 + threadIdx.x; g < g1; g += ST) occ += __ldcg(&R.slab[2 * g + 1]) != 0;
@@ -229,7 +272,10 @@ __global__ void __launch_bounds__(ST) k_serve(SHead* h, const SReq* __restrict__
       const long long c = local - R.npi - R.nch;
       if (threadIdx.x == 0) ok_s = wait_zero(&cnt[q].count_left, h, R.done);
       __syncthreads();
-      if (!ok_s) continue;
+      if (!ok_s) {
+        if (threadIdx.x == 0) item_s = (long long)(PF_PREFETCH_ITEMS ? next : atomicAdd(&h->counter, 1ULL));
+        continue;
+      }
       const long long* cc = chunk_counts + (long long)q * MAX_CHUNKS;
       long long base = 0, total = 0;
       for (long long k = 0; k < R.nch; ++k) {
@@ -274,6 +320,8 @@ __global__ void __launch_bounds__(ST) k_serve(SHead* h, const SReq* __restrict__
         }
       }
     }
+    __syncthreads();  // every thread has read item_s
+    if (threadIdx.x == 0) item_s = (long long)(PF_PREFETCH_ITEMS ? next : atomicAdd(&h->counter, 1ULL));
   }
   for (int o = 16; o; o >>= 1) {
     matched += __shfl_xor_sync(FULL, matched, o);
@@ -337,9 +385,9 @@ int staging_for(size_t bytes, Staging** out) {
   return PF_OK;
 }
 
-int serve_grid(int* grid) {
+int serve_grid(int* grid, size_t smem) {
   int per_sm = 0;
-  PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_serve, ST, 0));
+  PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_serve, ST, smem));
   *grid = std::max(1, per_sm) * sm_count();
   return PF_OK;
 }
@@ -388,7 +436,8 @@ extern "C" size_t pf_serve_workspace(int max_requests) {
 extern "C" int pf_serve_run(const pf_serve_request* reqs, int n, void* workspace,
                             size_t workspace_bytes, int64_t* stats, void* stream) {
   cudaStream_t st = (cudaStream_t)stream;
-  if (n < 1) return fail(PF_EINVAL, "serve_run: at least one request");
+  if (n < 1 || n > MAX_REQUESTS)
+    return fail(PF_EINVAL, "serve_run: 1 to %d requests a launch, got %d", MAX_REQUESTS, n);
   if (!stats) return fail(PF_EINVAL, "serve_run: null stats");
   Arena a(workspace, workspace_bytes);
   ServeLayout l = serve_layout(a, n);
@@ -437,6 +486,7 @@ extern "C" int pf_serve_run(const pf_serve_request* reqs, int n, void* workspace
     }
     R.lo = x.date_lo;
     R.hi = x.date_hi;
+    if (items > INT_MAX / 2) return fail(PF_EINVAL, "serve_run: too many work items");
     R.item0 = items;
     R.npi = (x.row_end - x.row_begin + PROBE_ROWS - 1) / PROBE_ROWS;
     R.nch = x.finish ? (x.n_groups + GROUP_CHUNK - 1) / GROUP_CHUNK : 0;
@@ -450,13 +500,14 @@ extern "C" int pf_serve_run(const pf_serve_request* reqs, int n, void* workspace
   H->n_req = n;
   H->error = 0;
   int grid = 0;
-  if (int rc = serve_grid(&grid)) return rc;
+  if (int rc = serve_grid(&grid, sizeof(int) * n)) return rc;
   PF_CUDA(cudaMemcpyAsync(l.head, img, bytes, cudaMemcpyHostToDevice, st));
   PF_CUDA(cudaEventRecord(stg->ev, st));
   stg->pending = true;
   {
     PF_KERNEL("k_serve", st);
-    k_serve<<<grid, ST, 0, st>>>(l.head, l.reqs, l.cnt, l.chunks, (unsigned long long*)stats);
+    k_serve<<<grid, ST, sizeof(int) * n, st>>>(l.head, l.reqs, l.cnt, l.chunks,
+                                                (unsigned long long*)stats);
   }
   PF_LAUNCH("k_serve");
   {
