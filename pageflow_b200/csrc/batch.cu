@@ -32,8 +32,40 @@ constexpr int BT2 = 256;
 #define PF_BATCH_BV 1
 #endif
 constexpr int BV = PF_BATCH_BV;  // rows a thread keeps in flight
+// 1: a probe item adds into the block's group cache (agg.cuh) and flushes it
+// at the item's end, so the hot groups of a skewed instance cost one global
+// atomic pair a block and item instead of one a warp and step; 0:
+// warp-combined global atomics only.
+#ifndef PF_BATCH_CACHE
+#define PF_BATCH_CACHE 1
+#endif
+// with the cache: 1 combine equal groups of a warp before the cache
+#ifndef PF_BATCH_CACHE_COMBINE
+#define PF_BATCH_CACHE_COMBINE 0
+#endif
+constexpr size_t BATCH_SMEM = PF_BATCH_CACHE ? sizeof(GroupCache) : 0;
+// Warp-combined add whose leaders go through the cache.
+__device__ __forceinline__ void combined_to(GroupCache& gc, unsigned long long* slab, long long g,
+                                            long long value) {
+  const unsigned act = __activemask();
+  const unsigned peers = __match_any_sync(act, g);
+  if (g < 0) return;
+  const unsigned long long v = (unsigned long long)value;
+  const unsigned s0 = __reduce_add_sync(peers, (unsigned)(v & 0x3fffff));
+  const unsigned s1 = __reduce_add_sync(peers, (unsigned)((v >> 22) & 0x3fffff));
+  const unsigned s2 = __reduce_add_sync(peers, (unsigned)(v >> 44));
+  if ((int)(threadIdx.x & 31) == __ffs(peers) - 1)
+    cache_add(gc, slab, g,
+              (unsigned long long)s0 + ((unsigned long long)s1 << 22) +
+                  ((unsigned long long)s2 << 44),
+              (unsigned long long)__popc(peers));
+}
+
 constexpr int BITEM = 4096;
-constexpr int PITEM = 8192;
+#ifndef PF_BATCH_PITEM
+#define PF_BATCH_PITEM 16384
+#endif
+constexpr int PITEM = PF_BATCH_PITEM;
 constexpr unsigned WAIT_LIMIT = 1u << 24;  // polls of a probe item's wait (x ~0.5 us)
 
 struct Desc {
@@ -134,6 +166,11 @@ __global__ void __launch_bounds__(BT2) k_batch(Header* h, const Desc* d, const i
   const unsigned epoch = h->epoch;
   const long long ni = h->n_items;
   unsigned long long matched = 0, bad_group = 0, overflow = 0;
+#if PF_BATCH_CACHE
+  extern __shared__ __align__(16) unsigned char batch_smem[];
+  GroupCache& gc = *reinterpret_cast<GroupCache*>(batch_smem);
+  cache_init(gc);
+#endif
   // With PF_PREFETCH_ITEMS, thread 0 takes the block's next item while the
   // block works on the current one (measured no faster, so off by default).
   // Items are taken in increasing order and an item waits only for items
@@ -262,8 +299,19 @@ __global__ void __launch_bounds__(BT2) k_batch(Header* h, const Desc* d, const i
           }
         }
 #pragma unroll
-        for (int k = 0; k < BV; ++k) combined_add(slabs + 2 * D.soff, g[k], g[k] >= 0 ? value[k] : 0);
+        for (int k = 0; k < BV; ++k) {
+#if PF_BATCH_CACHE && PF_BATCH_CACHE_COMBINE
+          combined_to(gc, slabs + 2 * D.soff, g[k], g[k] >= 0 ? value[k] : 0);
+#elif PF_BATCH_CACHE
+          if (g[k] >= 0) cache_add(gc, slabs + 2 * D.soff, g[k], (unsigned long long)value[k], 1ULL);
+#else
+          combined_add(slabs + 2 * D.soff, g[k], g[k] >= 0 ? value[k] : 0);
+#endif
+        }
       }
+#if PF_BATCH_CACHE
+      cache_flush(gc, slabs + 2 * D.soff);
+#endif
     }
     __syncthreads();  // every thread has read item_s
     if (threadIdx.x == 0) item_s = (long long)(PF_PREFETCH_ITEMS ? next : atomicAdd(&h->counter, 1ULL));
@@ -301,7 +349,8 @@ bool find_plan(void* ws, HostPlan* out) {
 // The persistent grid: every block resident at once.
 int batch_grid(int* grid) {
   int per_sm = 0;
-  PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch, BT2, 0));
+  if (int rc = opt_in_smem((const void*)k_batch, BATCH_SMEM)) return rc;
+  PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch, BT2, BATCH_SMEM));
   *grid = std::max(1, per_sm) * sm_count();
   return PF_OK;
 }
@@ -413,7 +462,7 @@ extern "C" int pf_batch_run(void* workspace, int64_t* stats, void* stream) {
   PF_LAUNCH("k_batch_reset");
   {
     PF_KERNEL("k_batch", st);
-    k_batch<<<grid, BT2, 0, st>>>(l.header, l.desc, l.imap, l.remaining, l.tables, l.slabs,
+    k_batch<<<grid, BT2, BATCH_SMEM, st>>>(l.header, l.desc, l.imap, l.remaining, l.tables, l.slabs,
                                   (unsigned long long*)stats);
   }
   PF_LAUNCH("k_batch");

@@ -116,12 +116,19 @@ void launch_end(cudaStream_t st) {
 int opt_in_smem(const void* fn, size_t bytes) {
   static std::mutex mu;
   static std::map<std::pair<const void*, int>, size_t> done;
-  if (bytes <= 48 * 1024) return PF_OK;
+  if (bytes == 0) return PF_OK;
   int dev = 0;
   PF_CUDA(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lock(mu);
   size_t& have = done[{fn, dev}];
   if (have >= bytes) return PF_OK;
+  // the limit covers dynamic + static shared memory
+  cudaFuncAttributes fa{};
+  PF_CUDA(cudaFuncGetAttributes(&fa, fn));
+  if (bytes + fa.sharedSizeBytes <= 48 * 1024) {
+    have = bytes;
+    return PF_OK;
+  }
   PF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
   have = bytes;
   return PF_OK;

@@ -35,9 +35,15 @@ namespace {
 
 constexpr int ST = 256;
 #ifndef PF_SERVE_SV
-#define PF_SERVE_SV 2
+#define PF_SERVE_SV 4
 #endif
 constexpr int SV = PF_SERVE_SV;  // probe rows a thread keeps in flight
+// 1: probe items add through the block's group cache (agg.cuh), flushed at
+// the item's end; 0: hot_add into the slab directly.
+#ifndef PF_SERVE_CACHE
+#define PF_SERVE_CACHE 1
+#endif
+constexpr size_t SERVE_CACHE_SMEM = PF_SERVE_CACHE ? sizeof(GroupCache) : 0;
 constexpr long long PROBE_ROWS = 16384;
 constexpr long long GROUP_CHUNK = 16384;
 constexpr long long MAX_CHUNKS = 256;  // groups <= 4M a request
@@ -164,7 +170,10 @@ __device__ __forceinline__ long long block_sum(long long v, long long* red) {
 __global__ void __launch_bounds__(ST) k_serve(SHead* h, const SReq* __restrict__ reqs,
                                               SCounters* cnt, long long* chunk_counts,
                                               unsigned long long* stats) {
-  extern __shared__ int first_item[];
+  extern __shared__ __align__(16) unsigned char serve_smem[];
+  GroupCache& gc = *reinterpret_cast<GroupCache*>(serve_smem);
+  int* first_item = reinterpret_cast<int*>(serve_smem + SERVE_CACHE_SMEM);
+  if (PF_SERVE_CACHE) cache_init(gc);
   __shared__ long long item_s;
   __shared__ int ok_s;
   __shared__ long long red[ST / 32];
@@ -173,7 +182,7 @@ __global__ void __launch_bounds__(ST) k_serve(SHead* h, const SReq* __restrict__
   const int n = h->n_req;
   for (int i = threadIdx.x; i < n; i += ST) first_item[i] = (int)reqs[i].item0;
   unsigned long long matched = 0, kept = 0;
-  Combiner comb;
+  long long hot = -1;  // the warp's hot group (hot_add)
   // With PF_PREFETCH_ITEMS, thread 0 takes the block's next item while the
   // block works on the current one (measured no faster, so off by default).
   // Items are taken in increasing order and an item waits only for items
@@ -242,8 +251,15 @@ __global__ void __launch_bounds__(ST) k_serve(SHead* h, const SReq* __restrict__
           value[k] = g[k] >= 0 ? R.value[i] : 0;
         }
 #pragma unroll
-        for (int k = 0; k < SV; ++k) adaptive_add(R.slab, g[k], value[k], comb);
+        for (int k = 0; k < SV; ++k) {
+          if (PF_SERVE_CACHE) {
+            if (g[k] >= 0) cache_add(gc, R.slab, g[k], (unsigned long long)value[k], 1ULL);
+          } else {
+            hot_add(R.slab, g[k], value[k], hot);
+          }
+        }
       }
+      if (PF_SERVE_CACHE) cache_flush(gc, R.slab);
       __syncthreads();
       if (threadIdx.x == 0) {
         __threadfence();
@@ -387,6 +403,7 @@ int staging_for(size_t bytes, Staging** out) {
 
 int serve_grid(int* grid, size_t smem) {
   int per_sm = 0;
+  if (int rc = opt_in_smem((const void*)k_serve, smem)) return rc;
   PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_serve, ST, smem));
   *grid = std::max(1, per_sm) * sm_count();
   return PF_OK;
@@ -500,13 +517,13 @@ extern "C" int pf_serve_run(const pf_serve_request* reqs, int n, void* workspace
   H->n_req = n;
   H->error = 0;
   int grid = 0;
-  if (int rc = serve_grid(&grid, sizeof(int) * n)) return rc;
+  if (int rc = serve_grid(&grid, SERVE_CACHE_SMEM + sizeof(int) * n)) return rc;
   PF_CUDA(cudaMemcpyAsync(l.head, img, bytes, cudaMemcpyHostToDevice, st));
   PF_CUDA(cudaEventRecord(stg->ev, st));
   stg->pending = true;
   {
     PF_KERNEL("k_serve", st);
-    k_serve<<<grid, ST, sizeof(int) * n, st>>>(l.head, l.reqs, l.cnt, l.chunks,
+    k_serve<<<grid, ST, SERVE_CACHE_SMEM + sizeof(int) * n, st>>>(l.head, l.reqs, l.cnt, l.chunks,
                                                 (unsigned long long*)stats);
   }
   PF_LAUNCH("k_serve");
