@@ -516,6 +516,21 @@ __device__ __forceinline__ ulonglong2 ld_slot(const Slot* p) {
   return __ldcg(reinterpret_cast<const ulonglong2*>(p));
 }
 
+// 1: the partitioned sides, read once, are loaded evict-first (ld.global.cs)
+// so that they do not push the round's tables and the slab out of L2; the
+// probe value then travels in a register instead of shared memory.
+#ifndef PF_STREAM_HINTS
+#define PF_STREAM_HINTS 1
+#endif
+template <typename T>
+__device__ __forceinline__ T stream_ld(const T* p) {
+#if PF_STREAM_HINTS
+  return __ldcs(p);
+#else
+  return *p;
+#endif
+}
+
 // Build one row.  A slot is free for this round when its tag (the high half
 // of the tagged word) is below the round's tag (tags grow round by round; the
 // table is zeroed once per call): an atomicMax of the tag claims it without a
@@ -525,8 +540,8 @@ __device__ __forceinline__ ulonglong2 ld_slot(const Slot* p) {
 __device__ __forceinline__ void build_row(const RoundArgs& a, const uint2* reg, long long i,
                                           unsigned long long& bad_group,
                                           unsigned long long& overflow) {
-  const unsigned long long key = (unsigned long long)a.bkey[i];
-  const long long g = (long long)a.bgrp[i] - a.group_min;
+  const unsigned long long key = (unsigned long long)stream_ld(a.bkey + i);
+  const long long g = (long long)stream_ld(a.bgrp + i) - a.group_min;
   uint32_t goff = 0xffffffffu;
   if (g >= 0 && g < a.n_groups) goff = (uint32_t)g;
   else ++bad_group;
@@ -600,7 +615,9 @@ constexpr int PUROWS = PT2 * PR;
 
 struct ProbeStage {
   ulonglong2 slot[PR][PT2];
+#if !PF_STREAM_HINTS
   long long val[PR][PT2];
+#endif
 };
 
 __device__ __forceinline__ void probe_unit(const RoundArgs& a, const uint2* reg, long long lo,
@@ -610,18 +627,31 @@ __device__ __forceinline__ void probe_unit(const RoundArgs& a, const uint2* reg,
   unsigned long long key[PR];
   unsigned pos[PR];
   uint2 rg[PR];
+#if PF_STREAM_HINTS
+  long long val[PR];
+#pragma unroll
+  for (int k = 0; k < PR; ++k) {
+    const long long i = lo + k * PT2 + tid;
+    key[k] = i < hi ? (unsigned long long)stream_ld(a.pfk + i) : 0ULL;
+    val[k] = i < hi ? stream_ld(a.pval + i) : 0;
+  }
+#endif
 #pragma unroll
   for (int k = 0; k < PR; ++k) {
     const long long i = lo + k * PT2 + tid;
     rg[k] = make_uint2(0u, 0u);
     if (i < hi) {
+#if !PF_STREAM_HINTS
       key[k] = (unsigned long long)a.pfk[i];
+#endif
       const uint64_t h = mix64(key[k]);
       rg[k] = region_of(a, reg, h);
       if (rg[k].y) {
         pos[k] = first_slot(h, a.logB, rg[k].y);
         cp_async16(&st.slot[k][tid], a.table + rg[k].x + pos[k]);
+#if !PF_STREAM_HINTS
         cp_async8(&st.val[k][tid], a.pval + i);
+#endif
       }
     }
   }
@@ -635,7 +665,11 @@ __device__ __forceinline__ void probe_unit(const RoundArgs& a, const uint2* reg,
       if (sl.x == key[k]) {
         const uint32_t g = (uint32_t)sl.y;
         if (g != 0xffffffffu) {
+#if PF_STREAM_HINTS
+          atomicAdd(&a.slab[2 * (unsigned long long)g], (unsigned long long)val[k]);
+#else
           atomicAdd(&a.slab[2 * (unsigned long long)g], (unsigned long long)st.val[k][tid]);
+#endif
           atomicAdd(&a.slab[2 * (unsigned long long)g + 1], 1ULL);
         }
         ++matched;
