@@ -141,6 +141,22 @@ int pf_join_unique_hash_static(const int64_t* build0, const int64_t* build1, int
                                int nkeys, int64_t* build_idx, int64_t* probe_idx,
                                int64_t* match_count, void* stream);
 
+/*
+ * Late materialization: rows idx[0, n) of ncols columns (up to 16) in one
+ * launch, replacing the per-column torch.index_select / index_with_null of
+ * the reference's join tail (operators/hashjoin.py:355-377,
+ * conversion.py:39-50).  Column c has row_bytes[c]-byte rows of
+ * elem_bytes[c]-byte elements (1, 2, 4, 8) and n_src rows.  With allow_null,
+ * an index equal to null_idx gives a row of null_elem[c] elements (the bit
+ * pattern of the column's null value, e.g. -64 as that dtype); an index
+ * outside [0, n_src) gives that row too and is counted in bad[0] (device
+ * int64, added to).  Queued only.
+ */
+int pf_gather(const void* const* cols_in, void* const* cols_out, const int* row_bytes,
+              const int* elem_bytes, const uint64_t* null_elem, int ncols, const int64_t* idx,
+              int64_t n, int64_t n_src, int allow_null, int64_t null_idx, int64_t* bad,
+              void* stream);
+
 /* Residual operators of a semi/anti summary, as build.v OP probe.v. */
 #define PF_OP_NONE 0
 #define PF_OP_NE 1

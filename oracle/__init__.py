@@ -340,3 +340,39 @@ def serve_request(dim_keys, dim_groups, n_groups: int, fk, date, value, date_lo:
                                 np.asarray(value)[keep], None, 1, 0, n_groups, B=16)
     occ = np.nonzero(c)[0]
     return occ.astype(np.int64), s[occ], c[occ]
+
+
+# ---- join semantics ------------------------------------------------------------
+
+def join_rows(left_key, right_key, join_type: str, keep=None):
+    """The output rows of PageFlow's join core call (operators/hashjoin.py:
+    293-356, 444-494) as (left row or -64, right row) pairs, sorted: inner =
+    every (l, r) with equal keys that `keep(l, r)` passes; right-semi = the
+    right rows with such a pair (left -64 dropped: left rows are empty);
+    right-anti = the right rows with none; right-outer = the inner pairs
+    plus every right row with none, its left side -64."""
+    lk = np.asarray(left_key)
+    rk = np.asarray(right_key)
+    order = np.argsort(lk, kind="stable")
+    sk = lk[order]
+    lo = np.searchsorted(sk, rk, "left")
+    hi = np.searchsorted(sk, rk, "right")
+    pairs = []
+    matched = np.zeros(rk.shape[0], bool)
+    for r in range(rk.shape[0]):
+        for j in range(lo[r], hi[r]):
+            l = int(order[j])
+            if keep is None or keep(l, r):
+                pairs.append((l, r))
+                matched[r] = True
+    if join_type == "inner":
+        out = pairs
+    elif join_type == "right-semi":
+        out = [(-64, r) for r in np.nonzero(matched)[0].tolist()]
+    elif join_type == "right-anti":
+        out = [(-64, r) for r in np.nonzero(~matched)[0].tolist()]
+    elif join_type == "right-outer":
+        out = pairs + [(-64, r) for r in np.nonzero(~matched)[0].tolist()]
+    else:
+        raise ValueError(join_type)
+    return sorted(out)

@@ -45,6 +45,7 @@ _SIGS = {
                                    _vp, _vp, _sz, _vp]),
     "pf_join_unique_hash_static": (_int, [_vp, _vp, _i64, _vp, _vp, _i64, _int, _vp, _vp, _vp,
                                           _vp]),
+    "pf_gather": (_int, [_vp, _vp, _vp, _vp, _vp, _int, _vp, _i64, _i64, _int, _i64, _vp, _vp]),
     "pf_join_semi_anti_workspace": (_sz, [_i64, _i64, _int]),
     "pf_join_semi_anti": (_int, [_vp, _i64, _vp, _i64, _vp, _vp, _int, _int, _vp,
                                  _vp, _vp, _sz, _vp]),

@@ -1,0 +1,132 @@
+// Late materialization after a join: the rows of several columns at one
+// index array, in one launch (the reference gathers each output column with
+// its own torch.index_select / index_with_null: operators/hashjoin.py:
+// 355-377, conversion.py:39-50).
+//
+// Output row i of column c is input row idx[i] of column c, or, where
+// idx[i] is the null sentinel and nulls are allowed, a row whose every
+// element is the column's null element.  An index outside [0, n_src) (and
+// not an allowed null) writes the null row too and is counted in bad[0], so
+// the kernel never reads out of bounds.  Each CTA copies one tile of rows of
+// one column (blockIdx.y), in the widest steps (16 bytes down to 1) that the
+// row width and the columns' alignment allow.
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace pf {
+namespace {
+
+constexpr int GT = 256;
+constexpr int GMAXC = 16;
+
+struct GatherArgs {
+  const unsigned char* in[GMAXC];
+  unsigned char* out[GMAXC];
+  int row_bytes[GMAXC];
+  unsigned long long null_elem[GMAXC];  // the null element's bit pattern
+  int esize[GMAXC];
+  int wsize[GMAXC];  // bytes a copy step: the widest of 16, 8, 4, 2, 1 that
+                     // divides the row and both base addresses
+  const long long* idx;
+  long long n, n_src;
+  long long null_idx;
+  int allow_null;
+  unsigned long long* bad;
+};
+
+template <typename W>
+__device__ __forceinline__ void copy_row(const GatherArgs& a, int c, long long i, long long j,
+                                         bool null_row) {
+  const int words = a.row_bytes[c] / (int)sizeof(W);
+  W* dst = reinterpret_cast<W*>(a.out[c] + i * a.row_bytes[c]);
+  if (!null_row) {
+    const W* src = reinterpret_cast<const W*>(a.in[c] + j * a.row_bytes[c]);
+    for (int w = 0; w < words; ++w) dst[w] = src[w];
+    return;
+  }
+  // the null row: the element's bytes repeated along the row
+  for (int w = 0; w < words; ++w) {
+    W pat;
+    unsigned char* pb = reinterpret_cast<unsigned char*>(&pat);
+    for (int b = 0; b < (int)sizeof(W); ++b)
+      pb[b] = (unsigned char)(a.null_elem[c] >> (8 * ((w * (int)sizeof(W) + b) % a.esize[c])));
+    dst[w] = pat;
+  }
+}
+
+__global__ void __launch_bounds__(GT) k_gather(GatherArgs a) {
+  const int c = blockIdx.y;
+  unsigned long long bad = 0;
+  for (long long i = (long long)blockIdx.x * GT + threadIdx.x; i < a.n;
+       i += (long long)gridDim.x * GT) {
+    const long long j = a.idx[i];
+    bool null_row = false;
+    if (a.allow_null && j == a.null_idx) {
+      null_row = true;
+    } else if (j < 0 || j >= a.n_src) {
+      null_row = true;
+      ++bad;
+    }
+    switch (a.wsize[c]) {
+      case 16: copy_row<uint4>(a, c, i, j, null_row); break;
+      case 8: copy_row<unsigned long long>(a, c, i, j, null_row); break;
+      case 4: copy_row<unsigned>(a, c, i, j, null_row); break;
+      case 2: copy_row<unsigned short>(a, c, i, j, null_row); break;
+      default: copy_row<unsigned char>(a, c, i, j, null_row); break;
+    }
+  }
+  if (c == 0) {
+    for (int o = 16; o; o >>= 1) bad += __shfl_xor_sync(FULL, bad, o);
+    if ((threadIdx.x & 31) == 0 && bad) atomicAdd(a.bad, bad);
+  }
+}
+
+}  // namespace
+}  // namespace pf
+
+using namespace pf;
+
+extern "C" int pf_gather(const void* const* cols_in, void* const* cols_out, const int* row_bytes,
+                         const int* elem_bytes, const uint64_t* null_elem, int ncols,
+                         const int64_t* idx, int64_t n, int64_t n_src, int allow_null,
+                         int64_t null_idx, int64_t* bad, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (ncols < 1 || ncols > GMAXC) return fail(PF_EINVAL, "gather: 1 to %d columns", GMAXC);
+  if (n < 0 || n_src < 0) return fail(PF_EINVAL, "gather: negative sizes");
+  if (!bad) return fail(PF_EINVAL, "gather: null bad counter");
+  GatherArgs a{};
+  for (int c = 0; c < ncols; ++c) {
+    const int e = elem_bytes[c];
+    if (row_bytes[c] < 1 || (e != 1 && e != 2 && e != 4 && e != 8) || row_bytes[c] % e)
+      return fail(PF_EINVAL, "gather: column %d: %d-byte rows of %d-byte elements", c,
+                  row_bytes[c], e);
+    if ((n > 0 && !cols_out[c]) || (n_src > 0 && !cols_in[c]))
+      return fail(PF_EINVAL, "gather: column %d is null", c);
+    a.in[c] = (const unsigned char*)cols_in[c];
+    a.out[c] = (unsigned char*)cols_out[c];
+    a.row_bytes[c] = row_bytes[c];
+    a.esize[c] = e;
+    a.null_elem[c] = null_elem ? null_elem[c] : 0ULL;
+    int w = 16;
+    while (w > 1 && (row_bytes[c] % w || (uintptr_t)cols_in[c] % w || (uintptr_t)cols_out[c] % w))
+      w >>= 1;
+    a.wsize[c] = w;
+  }
+  if (n == 0) return ok();
+  if (!idx) return fail(PF_EINVAL, "gather: null index");
+  a.idx = (const long long*)idx;
+  a.n = n;
+  a.n_src = n_src;
+  a.null_idx = null_idx;
+  a.allow_null = allow_null;
+  a.bad = (unsigned long long*)bad;
+  const unsigned gx = (unsigned)std::max<long long>(
+      1, std::min<long long>((n + GT - 1) / GT, (long long)sm_count() * 8));
+  {
+    PF_KERNEL("k_gather", st);
+    k_gather<<<dim3(gx, (unsigned)ncols), GT, 0, st>>>(a);
+  }
+  PF_LAUNCH("k_gather");
+  return ok();
+}
