@@ -259,6 +259,47 @@ int pf_groups_finish(const int64_t* sum, const int64_t* count, int64_t group_min
                      int64_t n_groups, int64_t* keys_out, int64_t* sums_out, int64_t* counts_out,
                      int64_t* host_out, void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- sorted runs of the two-pass aggregation -------------------------------- */
+/*
+ * Stable ascending sort of n int64 keys carrying int64 values (vals_in NULL:
+ * the row numbers): LSD radix sort over the key range; waits once (for the
+ * range).  Outputs n rows each.
+ */
+size_t pf_sort_pairs_workspace(int64_t n);
+int pf_sort_pairs(const int64_t* keys_in, const int64_t* vals_in, int64_t n, int64_t* keys_out,
+                  int64_t* vals_out, void* workspace, size_t workspace_bytes, void* stream);
+/*
+ * Value columns of the run primitives: kinds[q] 0 = integer, 1 = float;
+ * esizes[q] 4 or 8; widths[q] elements a row (a (rows, width) tensor);
+ * ops[q] 0 = sum, 1 = amax, 2 = amin (operators/sorted_run_merge.py
+ * MERGEABLE_OPS).  Up to 8 columns.
+ *
+ * reduce_tick_slice (operators/sorted_run_merge.py:62-92): the unique keys
+ * of keys[0, n) ascending into keys_out and, per value column, each key's
+ * rows reduced by its op (the first row starts the reduction, as
+ * include_self=False does) into vals_out[q] (n_unique rows).  *n_unique
+ * (host) gets the unique count; waits twice.  Integer sums wrap as int64;
+ * float sums are added in no fixed order.
+ */
+size_t pf_unique_reduce_workspace(int64_t n);
+int pf_unique_reduce(const int64_t* keys, int64_t n, int ncols, const void* const* vals_in,
+                     void* const* vals_out, const int* kinds, const int* esizes,
+                     const int* widths, const int* ops, int64_t* keys_out, int64_t* n_unique,
+                     void* workspace, size_t workspace_bytes, void* stream);
+/*
+ * merge_sorted_unique_runs_inplace (operators/sorted_run_merge.py:94-174),
+ * out of place: the union of the ascending unique runs run_keys[0, n_run)
+ * and tick_keys[0, n_tick) into out_keys (n_run + n_tick rows of room), a
+ * key in both taking op(run value, tick value); *n_out (host) gets the
+ * merged length; waits once.
+ */
+size_t pf_merge_sorted_runs_workspace(int64_t n_tick);
+int pf_merge_sorted_runs(const int64_t* run_keys, const void* const* run_vals, int64_t n_run,
+                         const int64_t* tick_keys, const void* const* tick_vals, int64_t n_tick,
+                         int ncols, const int* kinds, const int* esizes, const int* widths,
+                         const int* ops, int64_t* out_keys, void* const* out_vals, int64_t* n_out,
+                         void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---- compressed pages: decode on arrival, filter, partition ---------------- */
 /*
  * PFC1 pages (pageflow_b200/csrc/codec.h): a page holds up to 2^30 values of
