@@ -259,6 +259,25 @@ int pf_groups_finish(const int64_t* sum, const int64_t* count, int64_t group_min
                      int64_t n_groups, int64_t* keys_out, int64_t* sums_out, int64_t* counts_out,
                      int64_t* host_out, void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- hash route of the keyed aggregation (pass 1) --------------------------- */
+/*
+ * Each row's grouping hash (KeyedAggregate.pass1's linear hash,
+ * operators/aggregate.py:551-564): key column c has row_bytes[c]-byte rows,
+ * read as little-endian int64 words zero-padded to a multiple of 8 bytes
+ * (_pack_as_int64, :482-505); hash = sum over columns and words of word *
+ * coeffs[c][word], int64 wrap-around.  coeffs[c]: device int64[ceil(
+ * row_bytes[c] / 8)].  Up to 8 key columns.  Queued only.
+ */
+int pf_group_hash(const void* const* key_cols, const int* row_bytes, const int64_t* const* coeffs,
+                  int ncols, int64_t n, int64_t* hash_out, void* stream);
+/*
+ * Each hash's bucket among B (a power of two <= 4096): the top log2(B) bits
+ * of its mix64 (_bucket_ids, operators/aggregate.py:107-116), int32; and
+ * the rows per bucket into counts_out (device int64[B], overwritten).
+ */
+int pf_hash_buckets(const int64_t* hash, int64_t n, int B, int32_t* bucket_out,
+                    int64_t* counts_out, void* stream);
+
 /* ---- sorted runs of the two-pass aggregation -------------------------------- */
 /*
  * Stable ascending sort of n int64 keys carrying int64 values (vals_in NULL:
@@ -272,7 +291,7 @@ int pf_sort_pairs(const int64_t* keys_in, const int64_t* vals_in, int64_t n, int
  * Value columns of the run primitives: kinds[q] 0 = integer, 1 = float;
  * esizes[q] 4 or 8; widths[q] elements a row (a (rows, width) tensor);
  * ops[q] 0 = sum, 1 = amax, 2 = amin (operators/sorted_run_merge.py
- * MERGEABLE_OPS).  Up to 8 columns.
+ * MERGEABLE_OPS).  Up to 16 columns.
  *
  * reduce_tick_slice (operators/sorted_run_merge.py:62-92): the unique keys
  * of keys[0, n) ascending into keys_out and, per value column, each key's

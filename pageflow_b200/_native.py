@@ -70,6 +70,8 @@ _SIGS = {
                             _vp]),
     "pf_gen_batch_probe": (_int, [ctypes.c_uint64, _i64, _i64, _i64, _int, _vp, _vp, _vp, _vp,
                                   _vp]),
+    "pf_group_hash": (_int, [_vp, _vp, _vp, _int, _i64, _vp, _vp]),
+    "pf_hash_buckets": (_int, [_vp, _i64, _int, _vp, _vp, _vp]),
     "pf_sort_pairs_workspace": (_sz, [_i64]),
     "pf_sort_pairs": (_int, [_vp, _vp, _i64, _vp, _vp, _vp, _sz, _vp]),
     "pf_unique_reduce_workspace": (_sz, [_i64]),

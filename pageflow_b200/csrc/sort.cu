@@ -370,7 +370,7 @@ __global__ void __launch_bounds__(256) k_segreduce(const T* __restrict__ in, T* 
 
 // ---- merge of two ascending unique runs ----------------------------------------
 
-constexpr int MAXV = 8;  // value columns
+constexpr int MAXV = 16;  // value columns
 
 struct VCols {
   const void* a[MAXV];   // run values

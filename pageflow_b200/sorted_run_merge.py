@@ -31,8 +31,8 @@ _PLACE_CHUNK = 1 << 26  # accepted for the reference's interface; the merge is o
 def _describe(vals: Sequence[torch.Tensor], ops: Sequence[str], what: str):
     if len(vals) != len(ops):
         raise ValueError(f"{what}: {len(vals)} value columns, {len(ops)} ops")
-    if len(vals) > 8:
-        raise ValueError(f"{what}: at most 8 value columns")
+    if len(vals) > 16:
+        raise ValueError(f"{what}: at most 16 value columns")
     kinds, sizes, widths, opc = [], [], [], []
     for v, op in zip(vals, ops):
         if op not in _OP:
