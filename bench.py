@@ -908,6 +908,128 @@ def serve_cpu_baseline(spec, dims, fact, trace, seconds: float = 10.0):
                       f"{rows} probe rows, {t_run:.1f} s"}
 
 
+def run_kernels(args, world, rank, local_rank):
+    """The operator primitives beside the fused path, each timed with CUDA
+    events (median of `steps` runs after `warmup`) on inputs far above L2,
+    against the reference's plain torch form of the same operation, results
+    checked equal: the join tail's gather (two int64 columns at 100M random
+    indexes), the radix sort (100M int64 keys over 40 bits), reduce_tick_slice
+    (100M rows, 1M keys, two int64 sums), the merge of two 50M-key runs, and
+    the keyed pass 1's grouping hash (100M rows, int64 + int32 keys)."""
+    import torch
+    from pageflow_b200 import gather as G, keyed_aggregate as KA, sorted_run_merge as SRM
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    peak, peak_kind = measured_peak()
+    g = torch.Generator(device=dev).manual_seed(7)
+    n = 100_000_000
+
+    def timed(fn):
+        for _ in range(max(1, args.warmup)):
+            fn()
+        ts = []
+        for _ in range(max(1, args.steps)):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    out = {}
+    # gather
+    a = torch.randint(-(1 << 40), 1 << 40, (n,), device=dev, generator=g)
+    b = torch.randint(-(1 << 40), 1 << 40, (n,), device=dev, generator=g)
+    idx = torch.randint(0, n, (n,), device=dev, generator=g)
+    ours = G.index_select_many([a, b], idx)
+    same = all(torch.equal(x, torch.index_select(y, 0, idx)) for x, y in zip(ours, [a, b]))
+    ms = timed(lambda: G.index_select_many([a, b], idx))
+    ms_ref = timed(lambda: [torch.index_select(a, 0, idx), torch.index_select(b, 0, idx)])
+    byts = n * (8 + 2 * 16)
+    out["gather_2x_int64"] = {"ms": ms, "gbs": byts / ms / 1e6, "frac": byts / ms / 1e6 / peak,
+                              "torch_ms": ms_ref, "identical": same}
+    del ours
+    # radix sort
+    k = torch.randint(0, 1 << 40, (n,), device=dev, generator=g)
+    ko, vo = SRM.sort_pairs(k)
+    rs, ri = torch.sort(k, stable=True)
+    same = bool(torch.equal(ko, rs) and torch.equal(vo, ri))
+    ms = timed(lambda: SRM.sort_pairs(k))
+    ms_ref = timed(lambda: torch.sort(k, stable=True))
+    byts = n * 5 * 32  # 5 passes of 40 bits: 16 B read + 16 B written a key
+    out["radix_sort_40bit"] = {"ms": ms, "keys_per_s": n / ms * 1e3, "gbs": byts / ms / 1e6,
+                               "frac": byts / ms / 1e6 / peak, "torch_ms": ms_ref,
+                               "identical": same}
+    del ko, vo, rs, ri
+    # reduce_tick_slice
+    keys = torch.randint(0, 1 << 20, (n,), device=dev, generator=g)
+    v1 = torch.randint(-10**6, 10**6, (n,), device=dev, generator=g)
+    v2 = torch.randint(-10**6, 10**6, (n,), device=dev, generator=g)
+    u, (s1, s2) = SRM.reduce_tick_slice(keys, [v1, v2], ["sum", "sum"])
+
+    def torch_reduce():
+        uu, inv = torch.unique(keys, return_inverse=True)
+        r1 = torch.zeros(uu.numel(), dtype=torch.int64, device=dev)
+        r1.scatter_reduce_(0, inv, v1, reduce="sum", include_self=False)
+        r2 = torch.zeros(uu.numel(), dtype=torch.int64, device=dev)
+        r2.scatter_reduce_(0, inv, v2, reduce="sum", include_self=False)
+        return uu, r1, r2
+    tu, t1, t2 = torch_reduce()
+    same = bool(torch.equal(u, tu) and torch.equal(s1, t1) and torch.equal(s2, t2))
+    ms = timed(lambda: SRM.reduce_tick_slice(keys, [v1, v2], ["sum", "sum"]))
+    ms_ref = timed(torch_reduce)
+    out["reduce_tick_slice_1M_keys"] = {"ms": ms, "rows_per_s": n / ms * 1e3,
+                                        "torch_ms": ms_ref, "identical": same}
+    del u, s1, s2, tu, t1, t2
+    # merge of two unique runs
+    ra = torch.unique(torch.randint(0, 1 << 34, (n // 2,), device=dev, generator=g))
+    rb = torch.unique(torch.randint(0, 1 << 34, (n // 2,), device=dev, generator=g))
+    va, vb = torch.ones_like(ra), torch.ones_like(rb)
+    cap = ra.numel() + rb.numel()
+
+    def ours_merge():
+        kb = torch.empty(cap, dtype=torch.int64, device=dev)
+        vv = torch.empty(cap, dtype=torch.int64, device=dev)
+        kb[:ra.numel()], vv[:ra.numel()] = ra, va
+        m = SRM.merge_sorted_unique_runs_inplace(kb, [vv], ra.numel(), rb, [vb], ["sum"])
+        return kb[:m], vv[:m]
+    mk, mv = ours_merge()
+    uu, inv = torch.unique(torch.cat([ra, rb]), return_inverse=True)
+    same = bool(torch.equal(mk, uu) and torch.equal(mv, torch.bincount(inv)))
+    ms = timed(ours_merge)
+    out["merge_runs_2x50M"] = {"ms": ms, "keys_per_s": cap / ms * 1e3, "identical": same}
+    del mk, mv, uu, inv
+    # grouping hash
+    k1 = torch.randint(-(1 << 40), 1 << 40, (n,), device=dev, generator=g)
+    k2 = torch.randint(0, 1 << 30, (n,), device=dev, generator=g, dtype=torch.int32)
+    keys2 = [k1.unsqueeze(1), k2.unsqueeze(1)]
+    coeffs = KA.make_key_coeffs(keys2, dev)
+    h = KA.group_hash(keys2, coeffs)
+
+    def torch_hash():
+        return (k1 * coeffs[0][0]) + (k2.to(torch.int64) & 0xFFFFFFFF) * coeffs[1][0]
+    same = bool(torch.equal(h, torch_hash()))
+    ms = timed(lambda: KA.group_hash(keys2, coeffs))
+    ms_ref = timed(torch_hash)
+    byts = n * (8 + 4 + 8)
+    out["group_hash_int64_int32"] = {"ms": ms, "gbs": byts / ms / 1e6,
+                                     "frac": byts / ms / 1e6 / peak, "torch_ms": ms_ref,
+                                     "identical": same}
+    if rank == 0:
+        line = {"metric": "operator primitives: ms per call (median) and GB/s of algorithmic bytes",
+                "value": out["gather_2x_int64"]["gbs"], "unit": "GB/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": out["gather_2x_int64"]["ms"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+                "data": "synthetic (seeded, on the device, far above L2)",
+                "config": {"workload": "kernels", "rows": n, "peak_gbs": peak,
+                           "peak_source": peak_kind},
+                "kernels": out}
+        print(json.dumps(line), flush=True)
+
+
 def main(argv=None) -> int:
     args = parse_args(argv)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -915,7 +1037,7 @@ def main(argv=None) -> int:
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     mode = args.workload.split("/", 1)[0]
     if args.impl == "reference":
-        if mode in ("serve", "paged", "batch"):
+        if mode in ("serve", "paged", "batch", "kernels"):
             if rank == 0:
                 why = {"serve": "the serve workload's reference arm is its plain form per "
                                 "request, reported as plain_form of --workload serve",
@@ -923,12 +1045,15 @@ def main(argv=None) -> int:
                                 "reported as cpu_baseline of --workload paged",
                        "batch": "the batch workload's reference arm is the plain form per "
                                 "instance, reported as plain_form_per_instance of --workload "
-                                "batch"}[mode]
+                                "batch",
+                       "kernels": "the primitives' reference arm is their torch plain form, "
+                                  "reported as torch_ms of --workload kernels"}[mode]
                 print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
             return 0
         run_reference(args, workload(args.workload), world, rank)
         return 0
-    run = {"batch": run_batch, "serve": run_serve, "paged": run_paged}.get(mode)
+    run = {"batch": run_batch, "serve": run_serve, "paged": run_paged,
+           "kernels": run_kernels}.get(mode)
     w = None if run else workload(args.workload)
     if world > 1:
         import datetime

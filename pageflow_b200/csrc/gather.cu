@@ -7,9 +7,9 @@
 // idx[i] is the null sentinel and nulls are allowed, a row whose every
 // element is the column's null element.  An index outside [0, n_src) (and
 // not an allowed null) writes the null row too and is counted in bad[0], so
-// the kernel never reads out of bounds.  Each CTA copies one tile of rows of
-// one column (blockIdx.y), in the widest steps (16 bytes down to 1) that the
-// row width and the columns' alignment allow.
+// the kernel never reads out of bounds.  A thread copies one output row of
+// every column (the index read once), in the widest steps (16 bytes down to
+// 1) that the row width and the columns' alignment allow.
 #include <algorithm>
 
 #include "common.cuh"
@@ -32,8 +32,16 @@ struct GatherArgs {
   long long n, n_src;
   long long null_idx;
   int allow_null;
+  int ncols;
   unsigned long long* bad;
 };
+
+// Source reads through the read-only path (the columns do not change during
+// the launch).
+template <typename W>
+__device__ __forceinline__ W ldg_word(const W* p) { return __ldg(p); }
+template <>
+__device__ __forceinline__ uint4 ldg_word<uint4>(const uint4* p) { return __ldg(p); }
 
 template <typename W>
 __device__ __forceinline__ void copy_row(const GatherArgs& a, int c, long long i, long long j,
@@ -42,7 +50,7 @@ __device__ __forceinline__ void copy_row(const GatherArgs& a, int c, long long i
   W* dst = reinterpret_cast<W*>(a.out[c] + i * a.row_bytes[c]);
   if (!null_row) {
     const W* src = reinterpret_cast<const W*>(a.in[c] + j * a.row_bytes[c]);
-    for (int w = 0; w < words; ++w) dst[w] = src[w];
+    for (int w = 0; w < words; ++w) dst[w] = ldg_word(src + w);
     return;
   }
   // the null row: the element's bytes repeated along the row
@@ -55,8 +63,11 @@ __device__ __forceinline__ void copy_row(const GatherArgs& a, int c, long long i
   }
 }
 
+template <int NC>
 __global__ void __launch_bounds__(GT) k_gather(GatherArgs a) {
-  const int c = blockIdx.y;
+  // a thread takes one output row of every column: the index is read once
+  // and the columns' loads are in flight together
+  const int ncols = NC > 0 ? NC : a.ncols;
   unsigned long long bad = 0;
   for (long long i = (long long)blockIdx.x * GT + threadIdx.x; i < a.n;
        i += (long long)gridDim.x * GT) {
@@ -68,18 +79,20 @@ __global__ void __launch_bounds__(GT) k_gather(GatherArgs a) {
       null_row = true;
       ++bad;
     }
-    switch (a.wsize[c]) {
-      case 16: copy_row<uint4>(a, c, i, j, null_row); break;
-      case 8: copy_row<unsigned long long>(a, c, i, j, null_row); break;
-      case 4: copy_row<unsigned>(a, c, i, j, null_row); break;
-      case 2: copy_row<unsigned short>(a, c, i, j, null_row); break;
-      default: copy_row<unsigned char>(a, c, i, j, null_row); break;
+#pragma unroll
+    for (int c = 0; c < (NC > 0 ? NC : GMAXC); ++c) {
+      if (NC == 0 && c >= ncols) break;
+      switch (a.wsize[c]) {
+        case 16: copy_row<uint4>(a, c, i, j, null_row); break;
+        case 8: copy_row<unsigned long long>(a, c, i, j, null_row); break;
+        case 4: copy_row<unsigned>(a, c, i, j, null_row); break;
+        case 2: copy_row<unsigned short>(a, c, i, j, null_row); break;
+        default: copy_row<unsigned char>(a, c, i, j, null_row); break;
+      }
     }
   }
-  if (c == 0) {
-    for (int o = 16; o; o >>= 1) bad += __shfl_xor_sync(FULL, bad, o);
-    if ((threadIdx.x & 31) == 0 && bad) atomicAdd(a.bad, bad);
-  }
+  for (int o = 16; o; o >>= 1) bad += __shfl_xor_sync(FULL, bad, o);
+  if ((threadIdx.x & 31) == 0 && bad) atomicAdd(a.bad, bad);
 }
 
 }  // namespace
@@ -120,12 +133,19 @@ extern "C" int pf_gather(const void* const* cols_in, void* const* cols_out, cons
   a.n_src = n_src;
   a.null_idx = null_idx;
   a.allow_null = allow_null;
+  a.ncols = ncols;
   a.bad = (unsigned long long*)bad;
   const unsigned gx = (unsigned)std::max<long long>(
       1, std::min<long long>((n + GT - 1) / GT, (long long)sm_count() * 8));
   {
     PF_KERNEL("k_gather", st);
-    k_gather<<<dim3(gx, (unsigned)ncols), GT, 0, st>>>(a);
+    switch (ncols) {
+      case 1: k_gather<1><<<gx, GT, 0, st>>>(a); break;
+      case 2: k_gather<2><<<gx, GT, 0, st>>>(a); break;
+      case 3: k_gather<3><<<gx, GT, 0, st>>>(a); break;
+      case 4: k_gather<4><<<gx, GT, 0, st>>>(a); break;
+      default: k_gather<0><<<gx, GT, 0, st>>>(a); break;
+    }
   }
   PF_LAUNCH("k_gather");
   return ok();

@@ -75,53 +75,108 @@ __global__ void __launch_bounds__(RT) k_rs_hist(const long long* __restrict__ ke
   hist[(long long)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
 }
 
-__global__ void __launch_bounds__(RT) k_rs_scatter(const long long* __restrict__ kin,
+// Each warp takes a contiguous 512-key segment of the tile (16 keys a lane,
+// in registers) and counts its digits; the counts give every digit's place
+// in the tile (digit order) and each warp's place inside it; each warp puts
+// its keys there in order - a round of 32 keys at a time, a key's place its
+// digit's running count in the warp plus its rank among the round's equal
+// digits (eight ballots) - in shared memory; then the block writes the tile
+// out digit run by digit run, consecutive threads on consecutive rows.
+struct ScatterSmem {
+  long long sk[RTILE];
+  long long sv[RTILE];
+  int wcnt[RW][256];   // the warp's digit counts, then its running place
+  int wloc[RW][256];   // the warp's first place per digit in the tile
+  int tstart[256];     // the digit's first place in the tile
+  long long gbase[256];
+  int wsum[RW];
+};
+
+__global__ void __launch_bounds__(RT, 2) k_rs_scatter(const long long* __restrict__ kin,
                                                    const long long* __restrict__ vin, long long n,
                                                    long long kmin, int shift, int ntiles,
                                                    const long long* __restrict__ offsets,
                                                    long long* __restrict__ kout,
                                                    long long* __restrict__ vout) {
-  __shared__ int cnt[RW][256];
-  __shared__ int off[RW][256];
-  __shared__ long long base[256];
+  extern __shared__ __align__(16) unsigned char rs_smem[];
+  ScatterSmem& S = *reinterpret_cast<ScatterSmem*>(rs_smem);
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  base[tid] = offsets[(long long)tid * ntiles + blockIdx.x];
 #pragma unroll
-  for (int q = 0; q < RW; ++q) cnt[q][tid] = 0;
+  for (int q = 0; q < RW; ++q) S.wcnt[q][tid] = 0;
+  S.gbase[tid] = offsets[(long long)tid * ntiles + blockIdx.x];
+  __syncthreads();
+  constexpr int SEG = RTILE / RW;  // 512 keys a warp
+  const long long t0 = (long long)blockIdx.x * RTILE;
+  const long long s0 = t0 + (long long)w * SEG;
+  long long key[RITEMS], val[RITEMS];
+  int dig[RITEMS];
+#pragma unroll
+  for (int k = 0; k < RITEMS; ++k) {
+    const long long i = s0 + k * 32 + lane;
+    const bool valid = i < n;
+    key[k] = valid ? kin[i] : 0;
+    val[k] = valid ? (vin ? vin[i] : i) : 0;
+    dig[k] = valid ? digit_of(key[k], kmin, shift) : -1;
+    if (valid) atomicAdd(&S.wcnt[w][dig[k]], 1);
+  }
+  __syncthreads();
+  // thread tid owns digit tid: its total, the tile's exclusive scan over
+  // digits, then each warp's place
+  int tot = 0;
+#pragma unroll
+  for (int q = 0; q < RW; ++q) tot += S.wcnt[q][tid];
+  int incl = tot;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(FULL, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) S.wsum[w] = incl;
+  __syncthreads();
+  int pre = 0;
+#pragma unroll
+  for (int q = 0; q < RW; ++q) pre += q < w ? S.wsum[q] : 0;
+  const int start = pre + incl - tot;
+  S.tstart[tid] = start;
+  {
+    int b = start;
+#pragma unroll
+    for (int q = 0; q < RW; ++q) {
+      S.wloc[q][tid] = b;
+      b += S.wcnt[q][tid];
+      S.wcnt[q][tid] = 0;
+    }
+  }
   __syncthreads();
   const unsigned lt = (1u << lane) - 1u;
-  const long long t0 = (long long)blockIdx.x * RTILE;
+#pragma unroll
   for (int k = 0; k < RITEMS; ++k) {
-    const long long i = t0 + k * RT + tid;
-    const bool valid = i < n;
-    const long long key = valid ? kin[i] : 0;
-    const long long val = valid ? (vin ? vin[i] : i) : 0;
-    const int d = valid ? digit_of(key, kmin, shift) : 0;
+    const int d = dig[k];
+    const bool valid = d >= 0;
     unsigned peers = __ballot_sync(FULL, valid);
 #pragma unroll
     for (int b = 0; b < 8; ++b) {
       const unsigned bb = __ballot_sync(FULL, (d >> b) & 1);
       peers &= ((d >> b) & 1) ? bb : ~bb;
     }
-    const int rw = __popc(peers & lt);
-    if (valid && rw == 0) cnt[w][d] = __popc(peers);
-    __syncthreads();
-    int tot = 0;
-#pragma unroll
-    for (int q = 0; q < RW; ++q) {
-      const int c = cnt[q][tid];
-      cnt[q][tid] = 0;
-      off[q][tid] = tot;
-      tot += c;
-    }
-    __syncthreads();
+    const int before = __popc(peers & lt);
+    const int run = valid ? S.wcnt[w][d] : 0;
+    __syncwarp();
     if (valid) {
-      const long long pos = base[d] + off[w][d] + rw;
-      kout[pos] = key;
-      vout[pos] = val;
+      const int loc = S.wloc[w][d] + run + before;
+      S.sk[loc] = key[k];
+      S.sv[loc] = val[k];
+      if (before == 0) S.wcnt[w][d] = run + __popc(peers);
     }
-    __syncthreads();
-    base[tid] += tot;
+    __syncwarp();
+  }
+  __syncthreads();
+  const int cnt = (int)min((long long)RTILE, n - t0);
+  for (int e = tid; e < cnt; e += RT) {
+    const long long kk = S.sk[e];
+    const int d = digit_of(kk, kmin, shift);
+    const long long pos = S.gbase[d] + (e - S.tstart[d]);
+    kout[pos] = kk;
+    vout[pos] = S.sv[e];
   }
 }
 
@@ -203,6 +258,7 @@ int sort_pairs(const long long* kin, const long long* vin, long long n, long lon
     return PF_OK;
   }
   const int ntiles = (int)((n + RTILE - 1) / RTILE);
+  if (int rc = opt_in_smem((const void*)k_rs_scatter, sizeof(ScatterSmem))) return rc;
   const long long* sk = kin;
   const long long* sv = vin;
   for (int p = 0; p < passes; ++p) {
@@ -218,7 +274,8 @@ int sort_pairs(const long long* kin, const long long* vin, long long n, long lon
     if (int rc = scan_i64(l.hist, l.offs, 256LL * ntiles, false, nullptr, l.scratch, st)) return rc;
     {
       PF_KERNEL("k_rs_scatter", st);
-      k_rs_scatter<<<ntiles, RT, 0, st>>>(sk, sv, n, mm[0], 8 * p, ntiles, l.offs, dk, dv);
+      k_rs_scatter<<<ntiles, RT, sizeof(ScatterSmem), st>>>(sk, sv, n, mm[0], 8 * p, ntiles,
+                                                            l.offs, dk, dv);
     }
     PF_LAUNCH("k_rs_scatter");
     sk = dk;
