@@ -30,6 +30,9 @@
 // the round's tag, so the table is cleared once per call, not per round.
 // The bucket counts come to the host once, to plan the rounds.
 #include <algorithm>
+#include <climits>
+#include <cstddef>
+#include <string>
 #include <vector>
 
 #include "scan.cuh"
@@ -57,6 +60,11 @@ constexpr int PT2 = 256;           // threads of build / probe
 // Build rows a round's table half holds (1.2M: two whole partitions of the
 // 150M-row build at B = 256, whose scatter is far cheaper than B = 512's).
 constexpr long long ROUND_ROWS_DEFAULT = 1200 * 1024;
+// 1: the shared-memory join path by default (PF_JOIN_PATH=rounds|smem
+// chooses at run time)
+#ifndef PF_JOIN_PATH_DEFAULT
+#define PF_JOIN_PATH_DEFAULT 1
+#endif
 
 struct Slot {
   unsigned long long key;
@@ -126,8 +134,10 @@ __global__ void __launch_bounds__(FT) k_fscan(int* __restrict__ hist, int nchunk
 // ---- 3. the scatter ---------------------------------------------------------------
 
 // VAL: the carried value's type (int for the build side's group, long long for
-// the probe side's computed value).
-template <bool PROBE>
+// the probe side's computed value).  HASHED: each row carries mix64(key) in
+// place of its key (mix64 is a bijection, so equal keys are equal hashes; the
+// shared-memory join path reads buckets and slots from it directly).
+template <bool PROBE, bool HASHED>
 __global__ void __launch_bounds__(FT) k_fscatter(const long long* __restrict__ key,
                                                  const void* __restrict__ v0,
                                                  const long long* __restrict__ v1,
@@ -181,7 +191,9 @@ __global__ void __launch_bounds__(FT) k_fscatter(const long long* __restrict__ k
     for (int k = 0; k < FITEMS; ++k) {
       const long long i = sb + k * FT + tid;
       if (i < hi) {
-        bk[k] = bucket_of_hash(mix64((uint64_t)kv[k]), logB);
+        const uint64_t h = mix64((uint64_t)kv[k]);
+        if (HASHED) kv[k] = (long long)h;
+        bk[k] = bucket_of_hash(h, logB);
         rk[k] = atomicAdd(&cnt[bk[k]], 1);
       }
     }
@@ -308,7 +320,7 @@ struct TmaSmem {
   }
 };
 
-template <bool PROBE>
+template <bool PROBE, bool HASHED>
 __global__ void __launch_bounds__(TT) k_fscatter_tma(const long long* __restrict__ key,
                                                      const void* __restrict__ v0,
                                                      const long long* __restrict__ v1,
@@ -413,7 +425,9 @@ __global__ void __launch_bounds__(TT) k_fscatter_tma(const long long* __restrict
         } else {
           vv[k] = r < tv ? iv[r] : g0[sb + r];
         }
-        bk[k] = bucket_of_hash(mix64(kv[k]), logB);
+        const uint64_t h = mix64(kv[k]);
+        if (HASHED) kv[k] = h;
+        bk[k] = bucket_of_hash(h, logB);
         rk[k] = atomicAdd(&cnt[bk[k]], 1);
       }
     }
@@ -737,6 +751,773 @@ __global__ void __launch_bounds__(PT2, PF_PROBE_MINB) k_fround(RoundArgs pa, Rou
   if (overflow) atomicAdd(&ba.stats[3], overflow);
 }
 
+
+// ---- the shared-memory join: a second radix pass, then per sub-partition ----
+//
+// PF_JOIN_PATH=smem (or the default when it is the faster path): the first
+// scatter carries each key's mix64 hash in place of the key (a bijection:
+// equal keys, equal hashes), each partition is split again by the next
+// log2(B2) bits of the hash (k_p2_hist, k_p2_colsum, scan, k_p2_scatter), so
+// every sub-partition holds about SJ_TARGET build rows; then k_sjoin takes
+// sub-partitions from a counter: it puts the build rows into a shared-memory
+// table {hash, group offset, sum, count}, adds every matching probe row's
+// value and 1 into its build row's cell with shared-memory atomics, and
+// flushes each build row that matched into the group slab with one pair of
+// global REDs.  Per probe row no L2 operation at all; per build row one pair.
+// A sub-partition with more build rows than the table takes is joined in
+// table-sized chunks of its build rows, each chunk against all of its probe
+// rows.  The table marks a free slot with the hash INT64_MIN; the key whose
+// hash that is gets a cell of its own.
+
+constexpr int P2T = 512;
+constexpr int P2I = 8;
+constexpr int P2TILE = P2T * P2I;  // rows a pass-2 tile
+constexpr int P2MAXLOG = 10;       // sub-buckets a partition splits into, log2, at most
+constexpr int P2BINS = 1 << P2MAXLOG;
+static_assert(P2BINS == 2 * P2T, "two bins a thread in the tile scan");
+#ifndef PF_SJT
+#define PF_SJT 512
+#endif
+#ifndef PF_SJ_MINB
+#define PF_SJ_MINB 2
+#endif
+#ifndef PF_SJ_U
+#define PF_SJ_U 4
+#endif
+constexpr int SJT = PF_SJT;       // threads of the join
+#ifndef PF_SJ_LOGTS
+#define PF_SJ_LOGTS 12
+#endif
+constexpr int SJ_TS = 1 << PF_SJ_LOGTS;        // table slots
+constexpr int SJ_CAP = SJ_TS / 2;              // build rows a table takes
+constexpr long long SJ_TARGET = SJ_TS / 3;     // build rows a sub-partition aims at
+constexpr long long SJ_EMPTY = LLONG_MIN;
+constexpr unsigned SJ_NONE = 0xffffffffu;
+constexpr int SJ_U = PF_SJ_U;                  // probe rows a thread holds at once
+constexpr int SJ_BU = SJ_CAP / SJT;            // build rows a thread takes per chunk
+static_assert(SJ_CAP % SJT == 0, "whole build rounds");
+static_assert(SJ_TS < 0xffff, "slots fit the 16-bit slot index");
+
+// Pass 2 works on segments: runs of at most P2SEG rows inside one partition
+// (segment (p, j) is rows [start_p + j * P2SEG, min(start_p + (j + 1) * P2SEG,
+// end_p))), so a segment's rows share their partition and its 2^logB2
+// sub-buckets.
+constexpr long long P2SEG = 16LL * P2TILE;
+
+struct SegArgs {
+  const int2* seg;          // (partition, index in the partition)
+  int nseg;
+  const long long* pstart;  // the side's partition starts
+  const long long* pcnt;    // and rows
+  int logS, logB2;
+};
+
+__device__ __forceinline__ void seg_range(const SegArgs& g, int sg, long long& lo, long long& hi,
+                                          long long& base) {
+  const int2 d = g.seg[sg];
+  const long long p0 = g.pstart[d.x];
+  lo = p0 + (long long)d.y * P2SEG;
+  hi = min(lo + P2SEG, p0 + g.pcnt[d.x]);
+  base = (long long)d.x << g.logB2;
+}
+
+// Each segment's sub-bucket counts, hist[sg][b] (every one of the 2^logB2
+// written, zeros too).
+__global__ void __launch_bounds__(P2T) k_p2_hist(const long long* __restrict__ key, SegArgs g,
+                                                 int* __restrict__ hist) {
+  __shared__ int bins[P2BINS];
+  const int nb2 = 1 << g.logB2;
+  const int tid = threadIdx.x;
+  for (int sg = blockIdx.x; sg < g.nseg; sg += gridDim.x) {
+    long long lo, hi, base;
+    seg_range(g, sg, lo, hi, base);
+    for (int b = tid; b < nb2; b += P2T) bins[b] = 0;
+    __syncthreads();
+    for (long long t0 = lo; t0 < hi; t0 += P2TILE) {
+      long long kk[P2I];
+#pragma unroll
+      for (int q = 0; q < P2I; ++q) {
+        const long long i = t0 + q * P2T + tid;
+        kk[q] = i < hi ? stream_ld(key + i) : 0;
+      }
+#pragma unroll
+      for (int q = 0; q < P2I; ++q)
+        if (t0 + q * P2T + tid < hi)
+          atomicAdd(&bins[bucket_of_hash((uint64_t)kk[q], g.logS) - base], 1);
+    }
+    __syncthreads();
+    for (int b = tid; b < nb2; b += P2T) hist[(long long)sg * nb2 + b] = bins[b];
+  }
+}
+
+// Per sub-bucket (p, b), one thread: its rows, the sum of its count over the
+// partition's segments.
+__global__ void k_p2_colsum(const int* __restrict__ hist, const int* __restrict__ pseg, int S,
+                            int logB2, long long* __restrict__ tot) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= S) return;
+  const int p = idx >> logB2, b = idx & ((1 << logB2) - 1);
+  const int nb2 = 1 << logB2;
+  long long run = 0;
+  for (int sg = pseg[p]; sg < pseg[p + 1]; ++sg) run += hist[(long long)sg * nb2 + b];
+  tot[idx] = run;
+}
+
+template <typename V>
+struct P2Smem {
+  long long sk[P2TILE];
+  V sv[P2TILE];
+  int cnt[P2BINS];         // rows of a sub-bucket in the tile, then zero again
+  int lofs[P2BINS];        // a sub-bucket's first place in the tile
+  long long gpos[P2BINS];  // the sub-bucket's claimed first place in the output
+  int wsum[P2T / 32];
+};
+
+// Rows to their sub-bucket's run, tile by tile in row order across the grid
+// (so the blocks at work at one time all append to the same run ends, and
+// each output line fills while it is in L2): each row's rank in its
+// sub-bucket (a shared-memory atomic), the tile's exclusive scan over the
+// sub-buckets, one claim per sub-bucket on its global cursor (travelling
+// while the tile is staged in shared memory in sub-bucket order), then the
+// write-out with consecutive threads on consecutive places (runs of about
+// P2TILE / 2^logB2 rows).  The next tile's rows are loaded before the
+// write-out.  A tile's sub-buckets are those of its first row's partition; a
+// row of the next partition (tiles that straddle a boundary) claims a place
+// of its own.  Order inside a sub-bucket is not kept.
+template <typename V>
+__global__ void __launch_bounds__(P2T, 2) k_p2_scatter(const long long* __restrict__ key_in,
+                                                       const V* __restrict__ val_in, long long n,
+                                                       int logS, int logB2,
+                                                       unsigned long long* __restrict__ cursor,
+                                                       long long* __restrict__ key_out,
+                                                       V* __restrict__ val_out) {
+  extern __shared__ __align__(16) unsigned char p2_smem[];
+  P2Smem<V>& S = *reinterpret_cast<P2Smem<V>*>(p2_smem);
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int nb2 = 1 << logB2;
+  const long long ntiles = (n + P2TILE - 1) / P2TILE;
+  const int b0 = 2 * tid, b1 = 2 * tid + 1;  // the sub-buckets this thread scans
+  S.cnt[b0] = 0;
+  S.cnt[b1] = 0;
+  long long k[P2I];
+  V v[P2I];
+  long long tile = blockIdx.x;
+  auto load = [&](long long t) {
+#pragma unroll
+    for (int q = 0; q < P2I; ++q) {
+      const long long i = t * P2TILE + q * P2T + tid;
+      if (i < n) {
+        k[q] = stream_ld(key_in + i);
+        v[q] = stream_ld(val_in + i);
+      }
+    }
+  };
+  if (tile < ntiles) load(tile);
+  __syncthreads();
+  for (; tile < ntiles; tile += gridDim.x) {
+    const long long t0 = tile * P2TILE;
+    const long long base =
+        ((long long)bucket_of_hash((uint64_t)key_in[t0], logS) >> logB2) << logB2;
+    int slot[P2I];  // rank << P2MAXLOG | sub-bucket, or -1
+#pragma unroll
+    for (int q = 0; q < P2I; ++q) {
+      const long long i = t0 + q * P2T + tid;
+      slot[q] = -1;
+      if (i < n) {
+        const long long id = bucket_of_hash((uint64_t)k[q], logS);
+        const unsigned long long b = (unsigned long long)(id - base);
+        if (b < (unsigned long long)nb2) {
+          slot[q] = (atomicAdd(&S.cnt[b], 1) << P2MAXLOG) | (int)b;
+        } else {
+          const long long pos = (long long)atomicAdd(&cursor[id], 1ULL);
+          key_out[pos] = k[q];
+          val_out[pos] = v[q];
+        }
+      }
+    }
+    __syncthreads();
+    const int c0 = S.cnt[b0], c1 = S.cnt[b1];
+    const int s2 = c0 + c1;
+    int incl = s2;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) S.wsum[w] = incl;
+    S.cnt[b0] = 0;
+    S.cnt[b1] = 0;
+    __syncthreads();
+    int pre = 0, total = 0;
+#pragma unroll
+    for (int q = 0; q < P2T / 32; ++q) {
+      const int x = S.wsum[q];
+      pre += q < w ? x : 0;
+      total += x;
+    }
+    const int ex = pre + incl - s2;
+    S.lofs[b0] = ex;
+    S.lofs[b1] = ex + c0;
+    __syncthreads();
+    // the claims travel while the tile is placed
+    const long long g0 = c0 ? (long long)atomicAdd(&cursor[base + b0], (unsigned long long)c0) : 0;
+    const long long g1 = c1 ? (long long)atomicAdd(&cursor[base + b1], (unsigned long long)c1) : 0;
+#pragma unroll
+    for (int q = 0; q < P2I; ++q) {
+      if (slot[q] < 0) continue;
+      const int e = S.lofs[slot[q] & (P2BINS - 1)] + (slot[q] >> P2MAXLOG);
+      S.sk[e] = k[q];
+      S.sv[e] = v[q];
+    }
+    S.gpos[b0] = g0;
+    S.gpos[b1] = g1;
+    __syncthreads();
+    if (tile + gridDim.x < ntiles) load(tile + gridDim.x);
+    for (int e = tid; e < total; e += P2T) {
+      const long long key = S.sk[e];
+      const int b = (int)(bucket_of_hash((uint64_t)key, logS) - base);
+      const long long pos = S.gpos[b] + (e - S.lofs[b]);
+      key_out[pos] = key;
+      val_out[pos] = S.sv[e];
+    }
+    __syncthreads();
+  }
+}
+
+struct SJArgs {
+  const long long* bkey;
+  const int* bgrp;
+  const long long* pfk;
+  const long long* pval;
+  const unsigned long long* bstart;  // [S + 1]
+  const unsigned long long* pstart;  // [S + 1]
+  long long S;
+  int logS;
+  long long group_min, n_groups;
+  unsigned long long* slab;
+  unsigned long long* stats;
+  unsigned long long* counter;
+};
+
+// A cell's 64-bit sum in shared memory: with PF_SJ_SUM32, as two 32-bit
+// words added with 32-bit atomics (the low word's add returns its old value,
+// which shows the carry into the high word), else one 64-bit atomic add.
+#ifndef PF_SJ_SUM32
+#define PF_SJ_SUM32 1
+#endif
+struct SJSum {
+#if PF_SJ_SUM32
+  unsigned lo, hi;
+#else
+  unsigned long long v;
+#endif
+};
+__device__ __forceinline__ void sj_sum_add(SJSum& c, long long val) {
+#if PF_SJ_SUM32
+  const unsigned l = (unsigned)(unsigned long long)val;
+  const unsigned h = (unsigned)((unsigned long long)val >> 32);
+  const unsigned old = atomicAdd(&c.lo, l);
+  atomicAdd(&c.hi, h + (old + l < old ? 1u : 0u));
+#else
+  atomicAdd(&c.v, (unsigned long long)val);
+#endif
+}
+__device__ __forceinline__ unsigned long long sj_sum_get(const SJSum& c) {
+#if PF_SJ_SUM32
+  return ((unsigned long long)c.hi << 32) | c.lo;
+#else
+  return c.v;
+#endif
+}
+__device__ __forceinline__ void sj_sum_clear(SJSum& c) {
+#if PF_SJ_SUM32
+  c.lo = 0;
+  c.hi = 0;
+#else
+  c.v = 0;
+#endif
+}
+
+struct SJSmem {
+  long long key[SJ_TS];
+  SJSum sum[SJ_TS];
+  unsigned goff[SJ_TS];
+  unsigned cnt[SJ_TS];
+  unsigned short slot_of[SJ_CAP];  // the slot of each build row of the chunk
+  long long min_sum;               // the key hashing to INT64_MIN, kept apart
+  unsigned min_cnt, min_goff;
+  int has_min;
+  long long item;                  // the next sub-partition and its row ranges
+  long long bnd[4];
+};
+
+__device__ __forceinline__ unsigned sj_slot(uint64_t h, int logS) {
+  return (unsigned)((h << logS) >> (64 - PF_SJ_LOGTS));
+}
+
+// One probe row against the chunk's table: its value and 1 into the cell of
+// the build row with its key.
+__device__ __forceinline__ void sj_probe(SJSmem& S, long long key, long long val, int logS,
+                                         unsigned long long& matched) {
+  if (key == SJ_EMPTY) {
+    if (S.has_min) {
+      atomicAdd((unsigned long long*)&S.min_sum, (unsigned long long)val);
+      atomicAdd(&S.min_cnt, 1u);
+      ++matched;
+    }
+    return;
+  }
+  unsigned t = sj_slot((uint64_t)key, logS);
+  for (int probes = 0; probes < SJ_TS; ++probes) {
+    const long long x = S.key[t];
+    if (x == SJ_EMPTY) return;
+    if (x == key) {
+      sj_sum_add(S.sum[t], val);
+      atomicAdd(&S.cnt[t], 1u);
+      ++matched;
+      return;
+    }
+    t = (t + 1) & (SJ_TS - 1);
+  }
+}
+
+__global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
+  extern __shared__ __align__(16) unsigned char sj_smem[];
+  SJSmem& S = *reinterpret_cast<SJSmem*>(sj_smem);
+  const int tid = threadIdx.x;
+  for (int t = tid; t < SJ_TS; t += SJT) {
+    S.key[t] = SJ_EMPTY;
+    sj_sum_clear(S.sum[t]);
+    S.cnt[t] = 0;
+  }
+  unsigned long long matched = 0, bad_group = 0;
+  // thread 0 fetches the next sub-partition and its ranges while the block
+  // works on the current one
+  auto fetch = [&]() {
+    const long long n = (long long)atomicAdd(a.counter, 1ULL);
+    S.item = n;
+    if (n < a.S) {
+      S.bnd[0] = (long long)a.bstart[n];
+      S.bnd[1] = (long long)a.bstart[n + 1];
+      S.bnd[2] = (long long)a.pstart[n];
+      S.bnd[3] = (long long)a.pstart[n + 1];
+    }
+  };
+  if (tid == 0) fetch();
+  while (true) {
+    __syncthreads();
+    const long long s = S.item;
+    const long long b0 = S.bnd[0], b1 = S.bnd[1], p0 = S.bnd[2], p1 = S.bnd[3];
+    __syncthreads();
+    if (s >= a.S) break;
+    if (tid == 0) fetch();
+    if (b1 == b0 || p1 == p0) continue;
+    for (long long c0 = b0; c0 < b1; c0 += SJ_CAP) {
+      const int nb = (int)min((long long)SJ_CAP, b1 - c0);
+      if (tid == 0) {
+        S.has_min = 0;
+        S.min_sum = 0;
+        S.min_cnt = 0;
+      }
+      __syncthreads();
+      // build: each build row a slot of its own (all of a thread's rows
+      // loaded first)
+      long long bk[SJ_BU];
+      int bg[SJ_BU];
+#pragma unroll
+      for (int u = 0; u < SJ_BU; ++u) {
+        const int j = u * SJT + tid;
+        if (j < nb) {
+          bk[u] = stream_ld(a.bkey + c0 + j);
+          bg[u] = stream_ld(a.bgrp + c0 + j);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < SJ_BU; ++u) {
+        if (u * SJT + tid >= nb) continue;
+        const long long key = bk[u];
+        const long long g = (long long)bg[u] - a.group_min;
+        unsigned goff = SJ_NONE;
+        if (g >= 0 && g < a.n_groups) goff = (unsigned)g;
+        else ++bad_group;
+        if (key == SJ_EMPTY) {
+          S.has_min = 1;
+          S.min_goff = goff;
+          S.slot_of[u * SJT + tid] = 0xffff;
+          continue;
+        }
+        unsigned t = sj_slot((uint64_t)key, a.logS);
+        for (int probes = 0; probes < SJ_TS; ++probes) {
+          const long long old = (long long)atomicCAS((unsigned long long*)&S.key[t],
+                                                     (unsigned long long)SJ_EMPTY,
+                                                     (unsigned long long)key);
+          if (old == SJ_EMPTY) {
+            S.goff[t] = goff;
+            break;
+          }
+          t = (t + 1) & (SJ_TS - 1);
+        }
+        S.slot_of[u * SJT + tid] = (unsigned short)t;
+      }
+      __syncthreads();
+      // probe, SJ_U rows a thread in flight
+      for (long long i0 = p0; i0 < p1; i0 += (long long)SJT * SJ_U) {
+        long long key[SJ_U], val[SJ_U];
+#pragma unroll
+        for (int u = 0; u < SJ_U; ++u) {
+          const long long i = i0 + u * SJT + tid;
+          if (i < p1) {
+            key[u] = stream_ld(a.pfk + i);
+            val[u] = stream_ld(a.pval + i);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < SJ_U; ++u)
+          if (i0 + u * SJT + tid < p1) sj_probe(S, key[u], val[u], a.logS, matched);
+      }
+      __syncthreads();
+      // flush every build row that matched, and empty its slot
+      for (int j = tid; j < nb; j += SJT) {
+        const unsigned t = S.slot_of[j];
+        if (t == 0xffff) continue;
+        const unsigned c = S.cnt[t];
+        const unsigned go = S.goff[t];
+        if (c && go != SJ_NONE) {
+          atomicAdd(&a.slab[2 * (unsigned long long)go], sj_sum_get(S.sum[t]));
+          atomicAdd(&a.slab[2 * (unsigned long long)go + 1], (unsigned long long)c);
+        }
+        S.key[t] = SJ_EMPTY;
+        sj_sum_clear(S.sum[t]);
+        S.cnt[t] = 0;
+      }
+      if (tid == 0 && S.has_min && S.min_cnt && S.min_goff != SJ_NONE) {
+        atomicAdd(&a.slab[2 * (unsigned long long)S.min_goff], (unsigned long long)S.min_sum);
+        atomicAdd(&a.slab[2 * (unsigned long long)S.min_goff + 1], (unsigned long long)S.min_cnt);
+      }
+      __syncthreads();
+    }
+  }
+  for (int o = 16; o; o >>= 1) matched += __shfl_xor_sync(FULL, matched, o);
+  if ((tid & 31) == 0 && matched) atomicAdd(&a.stats[0], matched);
+  if (bad_group) atomicAdd(&a.stats[2], bad_group);
+}
+
+// ---- the staged join: k_sjoin with its rows brought in by bulk copies ----
+//
+// One block of SJST threads a SM.  Thread 0 is the producer: it takes
+// sub-partitions from the counter one ahead of the block, and issues bulk
+// copies (one mbarrier a buffer, bounded waits) of the next sub-partition's
+// build rows into the build buffer as soon as the current build is done, and
+// of probe pieces (SJ_PIECE rows) into two piece buffers as soon as one is
+// consumed, so the loads of the next rows travel while the block builds,
+// probes and flushes.  A copy starts on a 16-byte boundary: the range is
+// widened to whole 16-byte words (the arrays carry slack at their ends) and
+// the rows are read from their offset.  Build rows past the first SJ_CAP of a
+// sub-partition are joined chunk by chunk with direct loads, each chunk
+// against all of its probe rows.
+#ifndef PF_SJ_STAGED
+#define PF_SJ_STAGED 0
+#endif
+constexpr int SJST = 1024;
+constexpr int SJ_PIECE = 2048;
+constexpr int SJ_BSLACK = 8;  // build staging rows beyond SJ_CAP (widening to 4-row words)
+
+struct SJStage {
+  long long key[SJ_TS];
+  SJSum sum[SJ_TS];
+  unsigned goff[SJ_TS];
+  unsigned cnt[SJ_TS];
+  long long pk[2][SJ_PIECE + 2];
+  long long pv[2][SJ_PIECE + 2];
+  long long bk[SJ_CAP + SJ_BSLACK];
+  int bg[SJ_CAP + SJ_BSLACK];
+  unsigned short slot_of[SJ_CAP];
+  uint64_t bar[3];  // piece buffers 0 and 1, the build buffer
+  long long cur[5], nxt[5];  // sub-partition, build rows [b0, b1), probe rows [p0, p1)
+  long long min_sum;
+  unsigned min_cnt, min_goff;
+  int has_min;
+};
+static_assert(offsetof(SJStage, pk) % 16 == 0 && offsetof(SJStage, pv) % 16 == 0 &&
+                  offsetof(SJStage, bk) % 16 == 0 && offsetof(SJStage, bg) % 16 == 0 &&
+                  ((SJ_PIECE + 2) * 8) % 16 == 0 && offsetof(SJStage, bar) % 8 == 0,
+              "bulk copy destinations on 16-byte boundaries");
+
+// The next sub-partition with rows on both sides, or d[0] = -1.
+__device__ void sj_fetch(const SJArgs& a, long long* d) {
+  while (true) {
+    const long long n = (long long)atomicAdd(a.counter, 1ULL);
+    if (n >= a.S) {
+      d[0] = -1;
+      return;
+    }
+    const long long b0 = (long long)a.bstart[n], b1 = (long long)a.bstart[n + 1];
+    const long long p0 = (long long)a.pstart[n], p1 = (long long)a.pstart[n + 1];
+    if (b1 > b0 && p1 > p0) {
+      d[0] = n;
+      d[1] = b0;
+      d[2] = b1;
+      d[3] = p0;
+      d[4] = p1;
+      return;
+    }
+  }
+}
+
+__device__ __forceinline__ long long sj_pieces(const long long* d) {
+  return (d[4] - d[3] + SJ_PIECE - 1) / SJ_PIECE;
+}
+
+__device__ void sj_issue_build(SJStage& S, const SJArgs& a, const long long* d) {
+  const long long r0 = d[1], r1 = min(d[2], d[1] + SJ_CAP);
+  const long long lo = r0 & ~3LL, hi = (r1 + 3) & ~3LL;
+  const unsigned bk = (unsigned)((hi - lo) * 8), bg = (unsigned)((hi - lo) * 4);
+  mbar_arrive_expect_tx(&S.bar[2], bk + bg);
+  bulk_g2s(S.bk, a.bkey + lo, bk, &S.bar[2]);
+  bulk_g2s(S.bg, a.bgrp + lo, bg, &S.bar[2]);
+}
+
+__device__ void sj_issue_piece(SJStage& S, const SJArgs& a, const long long* d, long long k,
+                               int buf) {
+  const long long r0 = d[3] + k * SJ_PIECE, r1 = min(d[4], r0 + SJ_PIECE);
+  const long long lo = r0 & ~1LL, hi = (r1 + 1) & ~1LL;
+  const unsigned bytes = (unsigned)((hi - lo) * 8);
+  mbar_arrive_expect_tx(&S.bar[buf], 2 * bytes);
+  bulk_g2s(S.pk[buf], a.pfk + lo, bytes, &S.bar[buf]);
+  bulk_g2s(S.pv[buf], a.pval + lo, bytes, &S.bar[buf]);
+}
+
+// Producer state, thread 0's registers.
+struct SJProducer {
+  int unit;            // 0: issuing the current sub-partition's pieces, 1: the next one's
+  long long piece;     // the next piece of that unit
+  long long issued;    // pieces issued so far (piece i goes to buffer i & 1)
+  long long builds;    // build copies issued so far
+  // Issue pieces while a buffer is free (consumed: pieces taken so far).
+  __device__ void pump(SJStage& S, const SJArgs& a, long long consumed) {
+    while (issued < consumed + 2) {
+      const long long* d = unit == 0 ? S.cur : S.nxt;
+      if (d[0] < 0) return;
+      if (piece < sj_pieces(d)) {
+        sj_issue_piece(S, a, d, piece, (int)(issued & 1));
+        ++piece;
+        ++issued;
+      } else if (unit == 0) {
+        unit = 1;
+        piece = 0;
+      } else {
+        return;
+      }
+    }
+  }
+};
+
+__device__ __forceinline__ void sj_insert(SJStage& S, long long key, int grp, int j,
+                                          const SJArgs& a, unsigned long long& bad_group) {
+  const long long g = (long long)grp - a.group_min;
+  unsigned goff = SJ_NONE;
+  if (g >= 0 && g < a.n_groups) goff = (unsigned)g;
+  else ++bad_group;
+  if (key == SJ_EMPTY) {
+    S.has_min = 1;
+    S.min_goff = goff;
+    S.slot_of[j] = 0xffff;
+    return;
+  }
+  unsigned t = sj_slot((uint64_t)key, a.logS);
+  for (int probes = 0; probes < SJ_TS; ++probes) {
+    const long long old = (long long)atomicCAS((unsigned long long*)&S.key[t],
+                                               (unsigned long long)SJ_EMPTY,
+                                               (unsigned long long)key);
+    if (old == SJ_EMPTY) {
+      S.goff[t] = goff;
+      break;
+    }
+    t = (t + 1) & (SJ_TS - 1);
+  }
+  S.slot_of[j] = (unsigned short)t;
+}
+
+__device__ __forceinline__ void sj_lookup(SJStage& S, long long key, long long val, int logS,
+                                          unsigned long long& matched) {
+  if (key == SJ_EMPTY) {
+    if (S.has_min) {
+      atomicAdd((unsigned long long*)&S.min_sum, (unsigned long long)val);
+      atomicAdd(&S.min_cnt, 1u);
+      ++matched;
+    }
+    return;
+  }
+  unsigned t = sj_slot((uint64_t)key, logS);
+  for (int probes = 0; probes < SJ_TS; ++probes) {
+    const long long x = S.key[t];
+    if (x == SJ_EMPTY) return;
+    if (x == key) {
+      sj_sum_add(S.sum[t], val);
+      atomicAdd(&S.cnt[t], 1u);
+      ++matched;
+      return;
+    }
+    t = (t + 1) & (SJ_TS - 1);
+  }
+}
+
+// Every build row of the chunk that matched into the slab; the table emptied.
+// Ends with the block synchronised.
+__device__ __forceinline__ void sj_flush(SJStage& S, const SJArgs& a, int nb) {
+  const int tid = threadIdx.x;
+  for (int j = tid; j < nb; j += SJST) {
+    const unsigned t = S.slot_of[j];
+    if (t == 0xffff) continue;
+    const unsigned c = S.cnt[t];
+    const unsigned go = S.goff[t];
+    if (c && go != SJ_NONE) {
+      atomicAdd(&a.slab[2 * (unsigned long long)go], sj_sum_get(S.sum[t]));
+      atomicAdd(&a.slab[2 * (unsigned long long)go + 1], (unsigned long long)c);
+    }
+    S.key[t] = SJ_EMPTY;
+    sj_sum_clear(S.sum[t]);
+    S.cnt[t] = 0;
+  }
+  if (tid == 0) {
+    if (S.has_min && S.min_cnt && S.min_goff != SJ_NONE) {
+      atomicAdd(&a.slab[2 * (unsigned long long)S.min_goff], (unsigned long long)S.min_sum);
+      atomicAdd(&a.slab[2 * (unsigned long long)S.min_goff + 1], (unsigned long long)S.min_cnt);
+    }
+    S.has_min = 0;
+    S.min_sum = 0;
+    S.min_cnt = 0;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(SJST, 1) k_sjoin_staged(SJArgs a) {
+  extern __shared__ __align__(128) unsigned char sjs_smem[];
+  SJStage& S = *reinterpret_cast<SJStage*>(sjs_smem);
+  const int tid = threadIdx.x;
+  for (int t = tid; t < SJ_TS; t += SJST) {
+    S.key[t] = SJ_EMPTY;
+    sj_sum_clear(S.sum[t]);
+    S.cnt[t] = 0;
+  }
+  SJProducer pr{0, 0, 0, 0};
+  if (tid == 0) {
+    S.has_min = 0;
+    S.min_sum = 0;
+    S.min_cnt = 0;
+    for (int b = 0; b < 3; ++b) mbar_init(&S.bar[b], 1);
+    mbar_init_fence();
+    sj_fetch(a, S.cur);
+    if (S.cur[0] >= 0) {
+      sj_issue_build(S, a, S.cur);
+      pr.builds = 1;
+    }
+    sj_fetch(a, S.nxt);
+    pr.pump(S, a, 0);
+  }
+  __syncthreads();
+  unsigned long long matched = 0, bad_group = 0;
+  long long used = 0;   // pieces consumed
+  long long bused = 0;  // build buffers consumed
+  bool failed = false;
+  while (true) {
+    const long long s = S.cur[0];
+    const long long b0 = S.cur[1], b1 = S.cur[2], p0 = S.cur[3], p1 = S.cur[4];
+    if (s < 0) break;
+    // build the first chunk from the build buffer
+    const bool okb = mbar_wait_bounded(&S.bar[2], (unsigned)(bused & 1));
+    if (__syncthreads_or(!okb)) {
+      failed = true;
+      break;
+    }
+    ++bused;
+    const int nb0 = (int)min((long long)SJ_CAP, b1 - b0);
+    {
+      const int off = (int)(b0 & 3);
+      for (int j = tid; j < nb0; j += SJST)
+        sj_insert(S, S.bk[off + j], S.bg[off + j], j, a, bad_group);
+    }
+    __syncthreads();
+    if (tid == 0 && S.nxt[0] >= 0) {
+      fence_proxy_async_smem();
+      sj_issue_build(S, a, S.nxt);
+      ++pr.builds;
+    }
+    // probe the first chunk, piece by piece from the piece buffers
+    const long long np = sj_pieces(S.cur);
+    for (long long k = 0; k < np; ++k) {
+      const int buf = (int)(used & 1);
+      const bool okp = mbar_wait_bounded(&S.bar[buf], (unsigned)((used >> 1) & 1));
+      if (__syncthreads_or(!okp)) {
+        failed = true;
+        break;
+      }
+      const long long r0 = p0 + k * SJ_PIECE;
+      const int rows = (int)min((long long)SJ_PIECE, p1 - r0);
+      const int off = (int)(r0 & 1);
+      for (int i = tid; i < rows; i += SJST)
+        sj_lookup(S, S.pk[buf][off + i], S.pv[buf][off + i], a.logS, matched);
+      __syncthreads();
+      ++used;
+      if (tid == 0) {
+        fence_proxy_async_smem();
+        pr.pump(S, a, used);
+      }
+    }
+    if (failed) break;
+    // build rows past the first SJ_CAP: chunk by chunk, direct loads
+    int nb = nb0;
+    for (long long c0 = b0 + SJ_CAP; c0 < b1; c0 += SJ_CAP) {
+      sj_flush(S, a, nb);
+      nb = (int)min((long long)SJ_CAP, b1 - c0);
+      for (int j = tid; j < nb; j += SJST)
+        sj_insert(S, stream_ld(a.bkey + c0 + j), stream_ld(a.bgrp + c0 + j), j, a, bad_group);
+      __syncthreads();
+      for (long long i = p0 + tid; i < p1; i += SJST)
+        sj_lookup(S, stream_ld(a.pfk + i), stream_ld(a.pval + i), a.logS, matched);
+      __syncthreads();
+    }
+    sj_flush(S, a, nb);
+    // the next sub-partition becomes the current one
+    if (tid == 0) {
+      for (int q = 0; q < 5; ++q) S.cur[q] = S.nxt[q];
+      if (pr.unit == 1) {
+        pr.unit = 0;
+      } else {
+        pr.unit = 0;
+        pr.piece = 0;
+      }
+      if (S.cur[0] >= 0) sj_fetch(a, S.nxt);
+      else S.nxt[0] = -1;
+      fence_proxy_async_smem();
+      pr.pump(S, a, used);
+    }
+    __syncthreads();
+  }
+  if (failed) {
+    // a copy never landed: report it, let the copies in flight land, stop
+    if (tid == 0) {
+      atomicOr(&a.stats[1], 1ULL);
+      for (long long u = used; u < pr.issued; ++u)
+        mbar_wait_bounded(&S.bar[u & 1], (unsigned)((u >> 1) & 1), 1u << 16);
+      for (long long u = bused; u < pr.builds; ++u)
+        mbar_wait_bounded(&S.bar[2], (unsigned)(u & 1), 1u << 16);
+    }
+    __syncthreads();
+  }
+  for (int o = 16; o; o >>= 1) matched += __shfl_xor_sync(FULL, matched, o);
+  if ((tid & 31) == 0 && matched) atomicAdd(&a.stats[0], matched);
+  if (bad_group) atomicAdd(&a.stats[2], bad_group);
+}
+
+// PF_JOIN_PATH=rounds|smem picks the join path; read on every call (the
+// workspace size depends on it, so query and call must see the same value).
+int join_path_smem() {
+  const char* e = getenv("PF_JOIN_PATH");
+  if (e && std::string(e) == "rounds") return 0;
+  if (e && std::string(e) == "smem") return 1;
+  return PF_JOIN_PATH_DEFAULT;
+}
+
 // The interleaved slab split into the caller's sum and count arrays.
 __global__ void k_split(const unsigned long long* __restrict__ slab, long long n,
                         long long* __restrict__ sum, long long* __restrict__ count) {
@@ -856,6 +1637,21 @@ struct JaLayout {
   unsigned long long* slab;  // [2 * n_groups]: (sum, count) per group
   long long max_launches;
   unsigned* counters;        // [max_launches] work counters of the round launches
+  // the shared-memory path
+  long long s_max;           // sub-partitions at most
+  long long* pkey2;
+  int* pgrp2;
+  long long* pfk2;
+  long long* pval2;
+  long long nseg_max[2];       // pass-2 segments a side, at most
+  int2* seg2[2];               // the segments of each side
+  int* pseg2[2];               // [B + 1]: each partition's first segment
+  int* hist2[2];               // [segments][2^logB2]
+  unsigned long long* cur2;    // [2][s_max]: the pass-2 scatter's cursors
+  long long* tot2;             // [2][s_max]: rows per sub-partition
+  unsigned long long* start2;  // [2][s_max + 1]
+  long long* scan2;            // scan scratch
+  unsigned long long* sj_counter;
 };
 
 JaLayout ja_layout(Arena& a, long long nb, long long np, int B, long long n_groups) {
@@ -882,6 +1678,30 @@ JaLayout ja_layout(Arena& a, long long nb, long long np, int B, long long n_grou
   // slices of partitions over the budget, plus one
   l.max_launches = B + nb / std::max<long long>(1, l.table_slots / 2) + 2;
   l.counters = a.take<unsigned>(l.max_launches);
+  if (join_path_smem()) {
+    // a partition splits into at most 2^P2MAXLOG sub-partitions, and never
+    // finer than SJ_TARGET build rows
+    l.s_max = (long long)B * std::min<long long>(
+                                 P2BINS, (long long)pow2_at_least((uint64_t)(nb / SJ_TARGET + 1)));
+    // slack past the ends: the staged join's bulk copies widen their ranges
+    // to whole 16-byte words
+    l.pkey2 = a.take<long long>((size_t)nb + SJ_BSLACK);
+    l.pgrp2 = a.take<int>((size_t)nb + SJ_BSLACK);
+    l.pfk2 = a.take<long long>((size_t)np + 2);
+    l.pval2 = a.take<long long>((size_t)np + 2);
+    const long long rows[2] = {nb, np};
+    for (int side = 0; side < 2; ++side) {
+      l.nseg_max[side] = rows[side] / P2SEG + B + 1;
+      l.seg2[side] = a.take<int2>((size_t)l.nseg_max[side]);
+      l.pseg2[side] = a.take<int>((size_t)B + 1);
+      l.hist2[side] = a.take<int>((size_t)l.nseg_max[side] * P2BINS);
+    }
+    l.tot2 = a.take<long long>(2 * (size_t)l.s_max);
+    l.cur2 = a.take<unsigned long long>(2 * (size_t)l.s_max);
+    l.start2 = a.take<unsigned long long>(2 * ((size_t)l.s_max + 1));
+    l.scan2 = a.take<long long>(scan_scratch_elems(l.s_max));
+    l.sj_counter = a.take<unsigned long long>(1);
+  }
   return l;
 }
 
@@ -907,6 +1727,172 @@ long long* pinned_counts(size_t n) {
     have = n;
   }
   return buf;
+}
+
+
+// The first radix pass of both sides (the TMA-fed kernel when every column
+// is 16-byte aligned).
+template <bool HASHED>
+int fscatter_both(bool tma, const int64_t* build_key, const int32_t* build_group, long long n_build,
+                  const int64_t* probe_fk, const int64_t* probe_price, const int64_t* probe_disc,
+                  long long scale, long long n_probe, long long chunk_b, int nch_b,
+                  long long chunk_p, int nch_p, int logB, int B, const JaLayout& l,
+                  int64_t* stats_out, cudaStream_t st) {
+  if (tma) {
+    const size_t smb = tma_smem<false>(B), smp = tma_smem<true>(B);
+    if (int rc = opt_in_smem((const void*)k_fscatter_tma<false, HASHED>, smb)) return rc;
+    if (int rc = opt_in_smem((const void*)k_fscatter_tma<true, HASHED>, smp)) return rc;
+    {
+      PF_KERNEL("k_fscatter_build", st);
+      k_fscatter_tma<false, HASHED><<<nch_b, TT, smb, st>>>(
+          (const long long*)build_key, build_group, nullptr, 0, n_build, chunk_b, logB, B,
+          tma_nbuf<false>(B), l.hist_b, l.start, l.pkey, l.pgrp, (unsigned long long*)stats_out + 1);
+    }
+    {
+      PF_KERNEL("k_fscatter_probe", st);
+      k_fscatter_tma<true, HASHED><<<nch_p, TT, smp, st>>>(
+          (const long long*)probe_fk, probe_price, (const long long*)probe_disc, scale, n_probe,
+          chunk_p, logB, B, tma_nbuf<true>(B), l.hist_p, l.start + B, l.pfk, l.pval,
+          (unsigned long long*)stats_out + 1);
+    }
+  } else {
+    const size_t smb = fscatter_smem(B, false), smp = fscatter_smem(B, true);
+    if (int rc = opt_in_smem((const void*)k_fscatter<false, HASHED>, smb)) return rc;
+    if (int rc = opt_in_smem((const void*)k_fscatter<true, HASHED>, smp)) return rc;
+    {
+      PF_KERNEL("k_fscatter_build", st);
+      k_fscatter<false, HASHED><<<nch_b, FT, smb, st>>>((const long long*)build_key, build_group, nullptr, 0,
+                                                n_build, chunk_b, logB, B, l.hist_b, l.start, l.pkey,
+                                                l.pgrp);
+    }
+    {
+      PF_KERNEL("k_fscatter_probe", st);
+      k_fscatter<true, HASHED><<<nch_p, FT, smp, st>>>((const long long*)probe_fk, probe_price,
+                                               (const long long*)probe_disc, scale, n_probe, chunk_p,
+                                               logB, B, l.hist_p, l.start + B, l.pfk, l.pval);
+    }
+  }
+  return ok();
+}
+
+// The shared-memory path after the first scatter (counts on the host): the
+// second radix pass into sub-partitions of about SJ_TARGET build rows, the
+// join per sub-partition, the slab split.  Keys are mix64 hashes here.
+int join_smem(const JaLayout& l, int B, int logB, const long long* hc, long long n_build,
+              long long n_probe, long long group_min, long long n_groups, int64_t* sum_out,
+              int64_t* count_out, int64_t* stats_out, cudaStream_t st) {
+  long long maxp = 0;
+  for (int p = 0; p < B; ++p) maxp = std::max(maxp, hc[p]);
+  int logB2 = 0;
+  while ((maxp >> logB2) > SJ_TARGET && logB2 < P2MAXLOG &&
+         ((long long)B << (logB2 + 1)) <= l.s_max)
+    ++logB2;
+  const int logS = logB + logB2;
+  const long long S = 1LL << logS;
+  const int sms = sm_count();
+  unsigned long long* start[2] = {l.start2, l.start2 + l.s_max + 1};
+  SegArgs g[2];
+  for (int side = 0; side < 2; ++side) {
+    // the segments, from the partition rows on the host
+    std::vector<int2> seg;
+    std::vector<int> pseg((size_t)B + 1);
+    for (int p = 0; p < B; ++p) {
+      pseg[p] = (int)seg.size();
+      const long long n = hc[(size_t)side * B + p];
+      for (long long j = 0; j * P2SEG < n; ++j) seg.push_back(make_int2(p, (int)j));
+    }
+    pseg[B] = (int)seg.size();
+    if ((long long)seg.size() > l.nseg_max[side])
+      return fail(PF_ENOSPACE, "join_aggregate: %zu pass-2 segments, room for %lld",
+                  seg.size(), l.nseg_max[side]);
+    // pageable sources: the copies take the data before they return
+    if (!seg.empty())
+      PF_CUDA(cudaMemcpyAsync(l.seg2[side], seg.data(), seg.size() * sizeof(int2),
+                              cudaMemcpyHostToDevice, st));
+    PF_CUDA(cudaMemcpyAsync(l.pseg2[side], pseg.data(), pseg.size() * sizeof(int),
+                            cudaMemcpyHostToDevice, st));
+    g[side].seg = l.seg2[side];
+    g[side].nseg = (int)seg.size();
+    g[side].pstart = l.start + (size_t)side * B;
+    g[side].pcnt = l.cnt + (size_t)side * B;
+    g[side].logS = logS;
+    g[side].logB2 = logB2;
+    const long long* keys = side ? l.pfk : l.pkey;
+    if (g[side].nseg) {
+      PF_KERNEL("k_p2_hist", st);
+      k_p2_hist<<<(unsigned)std::min<long long>(g[side].nseg, sms * 4LL), P2T, 0, st>>>(
+          keys, g[side], l.hist2[side]);
+    }
+    PF_LAUNCH("k_p2_hist");
+    {
+      PF_KERNEL("k_p2_colsum", st);
+      k_p2_colsum<<<(unsigned)((S + 255) / 256), 256, 0, st>>>(
+          l.hist2[side], l.pseg2[side], (int)S, logB2, l.tot2 + side * l.s_max);
+    }
+    PF_LAUNCH("k_p2_colsum");
+    if (int rc = scan_i64(l.tot2 + side * l.s_max, (long long*)start[side], S, false,
+                          (long long*)start[side] + S, l.scan2, st))
+      return rc;
+    PF_CUDA(cudaMemcpyAsync(l.cur2 + side * l.s_max, start[side], S * sizeof(unsigned long long),
+                            cudaMemcpyDeviceToDevice, st));
+  }
+  {
+    const size_t sb = sizeof(P2Smem<int>), sp = sizeof(P2Smem<long long>);
+    if (int rc = opt_in_smem((const void*)k_p2_scatter<int>, sb)) return rc;
+    if (int rc = opt_in_smem((const void*)k_p2_scatter<long long>, sp)) return rc;
+    int ob = 0, op = 0;
+    PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ob, k_p2_scatter<int>, P2T, sb));
+    PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&op, k_p2_scatter<long long>, P2T, sp));
+    const unsigned gb = (unsigned)std::max<long long>(
+        1, std::min<long long>((n_build + P2TILE - 1) / P2TILE, (long long)std::max(1, ob) * sms));
+    const unsigned gp = (unsigned)std::max<long long>(
+        1, std::min<long long>((n_probe + P2TILE - 1) / P2TILE, (long long)std::max(1, op) * sms));
+    PF_KERNEL("k_p2_scatter", st);
+    k_p2_scatter<int><<<gb, P2T, sb, st>>>(l.pkey, l.pgrp, n_build, logS, logB2, l.cur2, l.pkey2,
+                                           l.pgrp2);
+    k_p2_scatter<long long><<<gp, P2T, sp, st>>>(l.pfk, l.pval, n_probe, logS, logB2,
+                                                 l.cur2 + l.s_max, l.pfk2, l.pval2);
+  }
+  PF_LAUNCH("k_p2_scatter");
+  unsigned long long* start_b = start[0];
+  unsigned long long* start_p = start[1];
+  SJArgs a{};
+  a.bkey = l.pkey2;
+  a.bgrp = l.pgrp2;
+  a.pfk = l.pfk2;
+  a.pval = l.pval2;
+  a.bstart = start_b;
+  a.pstart = start_p;
+  a.S = S;
+  a.logS = logS;
+  a.group_min = group_min;
+  a.n_groups = n_groups;
+  a.slab = l.slab;
+  a.stats = (unsigned long long*)stats_out;
+  a.counter = l.sj_counter;
+  PF_CUDA(cudaMemsetAsync(l.sj_counter, 0, sizeof(unsigned long long), st));
+  const char* se = getenv("PF_SJ_STAGED");
+  if (se ? se[0] != '0' : PF_SJ_STAGED) {
+    const size_t smem = sizeof(SJStage);
+    if (int rc = opt_in_smem((const void*)k_sjoin_staged, smem)) return rc;
+    PF_KERNEL("k_sjoin", st);
+    k_sjoin_staged<<<sms, SJST, smem, st>>>(a);
+  } else {
+    const size_t smem = sizeof(SJSmem);
+    if (int rc = opt_in_smem((const void*)k_sjoin, smem)) return rc;
+    int per_sm = 0;
+    PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sjoin, SJT, smem));
+    PF_KERNEL("k_sjoin", st);
+    k_sjoin<<<std::max(1, per_sm) * sms, SJT, smem, st>>>(a);
+  }
+  PF_LAUNCH("k_sjoin");
+  {
+    PF_KERNEL("k_split", st);
+    k_split<<<(unsigned)std::max<long long>(1, std::min<long long>((n_groups + 255) / 256, sms * 8LL)),
+              256, 0, st>>>(l.slab, n_groups, (long long*)sum_out, (long long*)count_out);
+  }
+  PF_LAUNCH("k_split");
+  return ok();
 }
 
 }  // namespace
@@ -1003,42 +1989,19 @@ extern "C" int pf_join_aggregate(const int64_t* build_key, const int32_t* build_
   const bool tma = aligned16(build_key) && aligned16(build_group) && aligned16(probe_fk) &&
                    aligned16(probe_price) && (!probe_disc || aligned16(probe_disc)) &&
                    getenv("PF_NO_TMA") == nullptr;
-  if (tma) {
-    const size_t smb = tma_smem<false>(B), smp = tma_smem<true>(B);
-    if (int rc = opt_in_smem((const void*)k_fscatter_tma<false>, smb)) return rc;
-    if (int rc = opt_in_smem((const void*)k_fscatter_tma<true>, smp)) return rc;
-    {
-      PF_KERNEL("k_fscatter_build", st);
-      k_fscatter_tma<false><<<nch_b, TT, smb, st>>>(
-          (const long long*)build_key, build_group, nullptr, 0, n_build, chunk_b, logB, B,
-          tma_nbuf<false>(B), l.hist_b, l.start, l.pkey, l.pgrp, (unsigned long long*)stats_out + 1);
-    }
-    {
-      PF_KERNEL("k_fscatter_probe", st);
-      k_fscatter_tma<true><<<nch_p, TT, smp, st>>>(
-          (const long long*)probe_fk, probe_price, (const long long*)probe_disc, scale, n_probe,
-          chunk_p, logB, B, tma_nbuf<true>(B), l.hist_p, l.start + B, l.pfk, l.pval,
-          (unsigned long long*)stats_out + 1);
-    }
-  } else {
-    const size_t smb = fscatter_smem(B, false), smp = fscatter_smem(B, true);
-    if (int rc = opt_in_smem((const void*)k_fscatter<false>, smb)) return rc;
-    if (int rc = opt_in_smem((const void*)k_fscatter<true>, smp)) return rc;
-    {
-      PF_KERNEL("k_fscatter_build", st);
-      k_fscatter<false><<<nch_b, FT, smb, st>>>((const long long*)build_key, build_group, nullptr, 0,
-                                                n_build, chunk_b, logB, B, l.hist_b, l.start, l.pkey,
-                                                l.pgrp);
-    }
-    {
-      PF_KERNEL("k_fscatter_probe", st);
-      k_fscatter<true><<<nch_p, FT, smp, st>>>((const long long*)probe_fk, probe_price,
-                                               (const long long*)probe_disc, scale, n_probe, chunk_p,
-                                               logB, B, l.hist_p, l.start + B, l.pfk, l.pval);
-    }
-  }
+  const bool smem_path = join_path_smem() != 0;
+  if (int rc = smem_path ? fscatter_both<true>(tma, build_key, build_group, n_build, probe_fk,
+                                                probe_price, probe_disc, scale, n_probe, chunk_b,
+                                                nch_b, chunk_p, nch_p, logB, B, l, stats_out, st)
+                         : fscatter_both<false>(tma, build_key, build_group, n_build, probe_fk,
+                                                 probe_price, probe_disc, scale, n_probe, chunk_b,
+                                                 nch_b, chunk_p, nch_p, logB, B, l, stats_out, st))
+    return rc;
   PF_LAUNCH("k_fscatter");
   if (int rc = wait_event(ev)) return rc;
+  if (join_path_smem())
+    return join_smem(l, B, logB, hc, n_build, n_probe, group_min, n_groups, sum_out, count_out,
+                     stats_out, st);
 
   // 4: plan the rounds from the counts
   const long long cap_rows = l.table_slots / 2;

@@ -8,7 +8,9 @@
   golden result from the reference's operators, against the oracle on random
   inputs (every fan-out, slices of a partition over the table budget, empty
   and ragged inputs, groups out of range, negative and extreme keys), and the
-  device generator against the CPU one.
+  device generator against the CPU one.  Every fused test runs on both join
+  paths (PF_JOIN_PATH=rounds: L2 tables in rounds; smem: a second radix pass
+  and shared-memory tables).
 """
 from __future__ import annotations
 
@@ -88,6 +90,12 @@ def test_slab_large_sum_is_exact_int64():
 
 # ---- the fused join -> group-by ---------------------------------------------------
 
+@pytest.fixture(params=["rounds", "smem"])
+def join_path(request, monkeypatch):
+    monkeypatch.setenv("PF_JOIN_PATH", request.param)
+    return request.param
+
+
 def _oracle_groups(bkey, bgrp, fk, price, disc, group_min, n_groups, scale=100):
     s, c, matched, _ = oracle.join_aggregate(
         bkey.cpu().numpy(), bgrp.cpu().numpy(), fk.cpu().numpy(), price.cpu().numpy(),
@@ -103,7 +111,7 @@ def _assert_groups(got, want):
     assert np.array_equal(counts.cpu().numpy(), want[2])
 
 
-def test_small_workload_is_the_references_result():
+def test_small_workload_is_the_references_result(join_path):
     """250K x 1M, seed 0: the groups, sums and counts of the reference's
     join + KeyedAggregate.pass1 + reduce_tick_slice."""
     g = load("config0.npz")
@@ -133,7 +141,7 @@ def test_device_generator_is_the_cpu_generator():
 
 
 @pytest.mark.parametrize("B", [1, 2, 16, 64, 256, 512, 1024, 4096])
-def test_every_fan_out_matches_the_oracle(B):
+def test_every_fan_out_matches_the_oracle(B, join_path):
     w = datagen.scaled(datagen.SCALE, 1 / 500)   # 300K x 1.2M, 3000 groups
     bkey, bgrp = datagen.gen_build(w, "cuda")
     fk, price, disc = datagen.gen_probe(w, "cuda")
@@ -144,7 +152,7 @@ def test_every_fan_out_matches_the_oracle(B):
     assert st.matched == want[3] and st.overflow == 0 and st.device_error == 0
 
 
-def test_partitions_over_the_table_budget_take_slices(monkeypatch):
+def test_partitions_over_the_table_budget_take_slices(monkeypatch, join_path):
     """B = 1 and 2 over 3M build rows: partitions over the 768K-row table
     budget, joined in slices, each probe row meeting every slice."""
     w = datagen.scaled(datagen.SCALE, 1 / 50)   # 3M x 12M
@@ -175,14 +183,14 @@ def _random_case(nb, np_, G, seed, gmin=0):
 @pytest.mark.parametrize("nb,np_,G", [(0, 10, 5), (10, 0, 5), (1, 1, 1), (3, 4097, 2),
                                       (4097, 3, 7), (50_000, 200_003, 1),
                                       (123_457, 654_321, 50_000)])
-def test_ragged_and_empty_inputs(nb, np_, G):
+def test_ragged_and_empty_inputs(nb, np_, G, join_path):
     bkey, bgrp, fk, price, disc = _random_case(nb, np_, G, nb + np_, gmin=-3)
     want = _oracle_groups(bkey, bgrp, fk, price, disc, -3, G)
     got = join_group_aggregate(bkey, bgrp, fk, price, disc, group_min=-3, n_groups=G, B=32)
     _assert_groups(got, want)
 
 
-def test_no_discount_column_and_another_scale():
+def test_no_discount_column_and_another_scale(join_path):
     bkey, bgrp, fk, price, disc = _random_case(20_000, 90_000, 100, 5)
     want = _oracle_groups(bkey, bgrp, fk, price, None, 0, 100)
     _assert_groups(join_group_aggregate(bkey, bgrp, fk, price, None, group_min=0, n_groups=100),
@@ -192,7 +200,7 @@ def test_no_discount_column_and_another_scale():
                                         n_groups=100), want)
 
 
-def test_groups_outside_the_range_are_counted_not_aggregated():
+def test_groups_outside_the_range_are_counted_not_aggregated(join_path):
     bkey, bgrp, fk, price, disc = _random_case(10_000, 40_000, 50, 6)
     plan = JoinAggregate(10_000, 40_000, 10, 20, "cuda", B=8)   # groups [10, 30) only
     keys, sums, counts = plan.run(bkey, bgrp, fk, price, disc)
@@ -202,7 +210,7 @@ def test_groups_outside_the_range_are_counted_not_aggregated():
     assert st.bad_groups == int(((bgrp < 10) | (bgrp >= 30)).sum())
 
 
-def test_repeated_runs_of_one_plan_are_identical():
+def test_repeated_runs_of_one_plan_are_identical(join_path):
     w = datagen.scaled(datagen.SCALE, 1 / 1000)
     bkey, bgrp = datagen.gen_build(w, "cuda")
     fk, price, disc = datagen.gen_probe(w, "cuda")
@@ -213,7 +221,7 @@ def test_repeated_runs_of_one_plan_are_identical():
             assert torch.equal(a, b)
 
 
-def test_scale_workload_tenth_matches_the_generator_expectation():
+def test_scale_workload_tenth_matches_the_generator_expectation(join_path):
     """A tenth of the 150M x 600M workload (15M x 60M, 150K groups) against
     the exact expectation from the generator (every group's sum and count)."""
     w = datagen.scaled(datagen.SCALE, 1 / 10)
@@ -225,3 +233,56 @@ def test_scale_workload_tenth_matches_the_generator_expectation():
     assert np.array_equal(plan.sum.cpu().numpy(), s)
     assert np.array_equal(plan.count.cpu().numpy(), c)
     assert plan.read_stats().matched == m
+
+
+def test_sub_partition_over_the_shared_table_is_joined_in_chunks(join_path):
+    """Build keys chosen so that the top 3 bits of their mix64 agree: at
+    B = 1 the second pass cannot split them below one sub-partition of ~10K
+    build rows, over the shared-memory table's capacity, so it is joined in
+    table-sized chunks of build rows, each against every probe row."""
+    g = torch.Generator().manual_seed(11)
+    cand = torch.randint(-(1 << 62), 1 << 62, (80_000,), generator=g).numpy()
+    top = oracle.mix64(cand) >> np.uint64(61)
+    bkey = torch.from_numpy(np.unique(cand[top == 0])).cuda()
+    nb = bkey.numel()
+    assert nb > 8_000
+    bgrp = torch.randint(0, 300, (nb,), generator=g, dtype=torch.int32).cuda()
+    pick = torch.randint(0, nb, (200_000,), generator=g).cuda()
+    fk = torch.where(torch.rand(200_000, generator=g).cuda() < 0.1, bkey[pick] + 1, bkey[pick])
+    price = torch.randint(-(1 << 30), 1 << 30, (200_000,), generator=g).cuda()
+    disc = torch.randint(0, 11, (200_000,), generator=g).cuda()
+    want = _oracle_groups(bkey, bgrp, fk, price, disc, 0, 300)
+    plan = JoinAggregate(nb, 200_000, 0, 300, "cuda", B=1)
+    _assert_groups(plan.run(bkey, bgrp, fk, price, disc), want)
+    assert plan.read_stats().matched == want[3]
+
+
+def _unmix64(h: int) -> int:
+    """The key whose mix64 is h (each step of the finalizer inverted)."""
+    M = (1 << 64) - 1
+    h ^= h >> 33
+    h = (h * pow(0xc4ceb9fe1a85ec53, -1, 1 << 64)) & M
+    h ^= h >> 33
+    h = (h * pow(0xff51afd7ed558ccd, -1, 1 << 64)) & M
+    h ^= h >> 33
+    return h - (1 << 64) if h >> 63 else h
+
+
+def test_extreme_keys_join(join_path):
+    """INT64_MIN and INT64_MAX as keys on both sides, and the key whose mix64
+    is 2^63 (the shared-memory table's free mark among hashes), beside
+    ordinary keys."""
+    I = np.iinfo(np.int64)
+    ks = _unmix64(1 << 63)
+    assert int(oracle.mix64(np.array([ks], np.int64))[0]) == 1 << 63
+    bkey = torch.tensor([I.min, I.max, 0, -1, 5, I.min + 1, ks], dtype=torch.int64).cuda()
+    bgrp = torch.tensor([0, 1, 2, 3, 4, 5, 6], dtype=torch.int32).cuda()
+    fk = torch.tensor([I.min, I.min, I.max, 7, -1, I.min + 1, 0, I.min, ks, ks, ks + 1],
+                      dtype=torch.int64).cuda()
+    price = torch.arange(1, 12, dtype=torch.int64).cuda() * 1000
+    disc = torch.zeros(11, dtype=torch.int64).cuda()
+    want = _oracle_groups(bkey, bgrp, fk, price, disc, 0, 7)
+    for B in (1, 4):
+        plan = JoinAggregate(7, 11, 0, 7, "cuda", B=B)
+        _assert_groups(plan.run(bkey, bgrp, fk, price, disc), want)
+        assert plan.read_stats().matched == want[3] == 9
