@@ -245,14 +245,21 @@ def algorithmic_bytes(w, B_rounds):
     columns each pass must read and write once.  k_fhist reads each side's
     keys; the scatters read the source columns and write the carried ones
     (build: key 8 + group 4; probe: fk 8 + value 8, from fk, price and
-    discount); the rounds (k_fround: build round r + 1 while probing round
-    r) read the partitioned sides once (build 12 B, probe 16 B a row); the
-    finish reads the 16-byte slab and writes the groups it keeps."""
+    discount).  Shared-memory path: k_p2_hist reads both sides' keys, the
+    second scatter reads and writes the carried columns (build 12 + 12,
+    probe 16 + 16 a row), k_sjoin reads the sub-partitioned sides once
+    (build 12 B, probe 16 B a row).  L2-round path: k_fround (build round
+    r + 1 while probing round r) reads the partitioned sides once.  The
+    finish reads the 16-byte slab and writes the groups it keeps.  A step
+    counts the kernels it ran."""
     nb, npr, g = w.n_build, w.n_probe, w.n_groups
     return {
         "k_fhist": 8 * (nb + npr),
         "k_fscatter_build": nb * (12 + 12),
         "k_fscatter_probe": npr * (24 + 16),
+        "k_p2_hist": 8 * (nb + npr),
+        "k_p2_scatter": nb * (12 + 12) + npr * (16 + 16),
+        "k_sjoin": nb * 12 + npr * 16,
         "k_fround": nb * 12 + npr * 16,
         "k_gcount": g * 8,
         "k_gemit": g * 16 + g * 24,
@@ -348,7 +355,7 @@ def run_ours(args, w, world, rank, local_rank):
         roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                     "bytes_per_launch": bytes_launch, "peak_source": peak_kind}
-    step_bytes = sum(alg.values())
+    step_bytes = sum(b for name, b in alg.items() if name in prof)
     step_gbs = step_bytes / (ms / args.steps / 1e3) / 1e9
     step_roofline = {"bound": "hbm", "algorithmic_bytes": step_bytes, "achieved": step_gbs,
                      "peak": peak, "unit": "GB/s", "frac": step_gbs / peak,
