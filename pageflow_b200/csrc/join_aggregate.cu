@@ -6,7 +6,7 @@
 // It replaces the reference's composition of partition_sort per morsel ->
 // join_unique_hash per bucket pair -> index_select -> KeyedAggregate.pass1 ->
 // reduce_tick_slice (uvm/join.py:98-225, uvm/aggregate.py:147-212), whose
-// every step is an HBM round trip, with four passes:
+// every step is an HBM round trip, with these passes:
 //
 //   1. k_fhist      per-chunk bucket histograms of both sides' keys
 //   2. k_fscan      per bucket, each chunk's offset (then the bucket starts)
@@ -14,13 +14,21 @@
 //                   side carries (fk, value) with value = price * (scale -
 //                   disc) computed on the way, so the price and discount
 //                   columns are read once and never written
-//   4. k_fround     per round, the round's build rows go into an
+//   then one of two joins (PF_JOIN_PATH):
+//   4s. smem (the default): the keys leave pass 3 as their mix64 hashes; a
+//                   second radix pass (k_p2_hist, k_p2_colsum, k_p2_scatter)
+//                   splits every partition into sub-partitions of about 1.4K
+//                   build rows, and k_sjoin joins each in a shared-memory
+//                   table, adding every matched probe row's value and 1 into
+//                   its build row's cell and flushing each build row once
+//                   into the dense group slab (sum, count)
+//   4r. rounds:     per round, the round's build rows go into an
 //                   open-addressing table in L2 (16-byte slots {key, group |
 //                   round tag}); each probe row of the round's partitions
-//                   looks its key up and adds its value and 1 into the dense
-//                   group slab (sum, count) with fire-and-forget atomics.  One
-//                   launch probes round r while it builds round r + 1 into
-//                   the other half of a double-buffered table
+//                   looks its key up and adds its value and 1 into the slab
+//                   with fire-and-forget atomics.  One launch probes round r
+//                   while it builds round r + 1 into the other half of a
+//                   double-buffered table
 //
 // A row's bucket is the top log2(B) bits of mix64(key), as in the reference's
 // partition kernel.  A round is a run of whole partitions whose build rows fit
@@ -28,7 +36,8 @@
 // load <= 0.5), or one slice of a partition too large for it (its probe rows
 // then meet every slice; a unique build key lives in exactly one).  Slots carry
 // the round's tag, so the table is cleared once per call, not per round.
-// The bucket counts come to the host once, to plan the rounds.
+// The bucket counts come to the host once, to plan the rounds or the
+// sub-partitions.
 #include <algorithm>
 #include <climits>
 #include <cstddef>
