@@ -778,12 +778,25 @@ __global__ void __launch_bounds__(PT2, PF_PROBE_MINB) k_fround(RoundArgs pa, Rou
 // rows.  The table marks a free slot with the hash INT64_MIN; the key whose
 // hash that is gets a cell of its own.
 
-constexpr int P2T = 512;
-constexpr int P2I = 8;
+// One 1024-thread block a SM with 8192-row tiles: runs of 16 rows at 512
+// sub-buckets (measured against 512 threads x 4096 rows: 6.03 vs 6.79 ms for
+// the 150M x 600M second pass).
+#ifndef PF_P2T
+#define PF_P2T 1024
+#endif
+#ifndef PF_P2I
+#define PF_P2I 8
+#endif
+#ifndef PF_P2_MINB
+#define PF_P2_MINB 1
+#endif
+constexpr int P2T = PF_P2T;
+constexpr int P2I = PF_P2I;
 constexpr int P2TILE = P2T * P2I;  // rows a pass-2 tile
 constexpr int P2MAXLOG = 10;       // sub-buckets a partition splits into, log2, at most
 constexpr int P2BINS = 1 << P2MAXLOG;
-static_assert(P2BINS == 2 * P2T, "two bins a thread in the tile scan");
+constexpr int P2BPT = P2BINS / P2T;  // sub-buckets a thread scans
+static_assert(P2BINS % P2T == 0 && P2BPT >= 1, "whole sub-buckets a thread in the tile scan");
 #ifndef PF_SJT
 #define PF_SJT 512
 #endif
@@ -792,6 +805,11 @@ static_assert(P2BINS == 2 * P2T, "two bins a thread in the tile scan");
 #endif
 #ifndef PF_SJ_U
 #define PF_SJ_U 4
+#endif
+// 1: sub-partitions taken in turn by block index (their ranges loaded one
+// sub-partition ahead), 0: from a shared counter
+#ifndef PF_SJ_STATIC
+#define PF_SJ_STATIC 0
 #endif
 constexpr int SJT = PF_SJT;       // threads of the join
 #ifndef PF_SJ_LOGTS
@@ -893,9 +911,18 @@ struct P2Smem {
 // write-out.  A tile's sub-buckets are those of its first row's partition; a
 // row of the next partition (tiles that straddle a boundary) claims a place
 // of its own.  Order inside a sub-bucket is not kept.
-template <typename V>
-__global__ void __launch_bounds__(P2T, 2) k_p2_scatter(const long long* __restrict__ key_in,
-                                                       const V* __restrict__ val_in, long long n,
+//
+// MODE 0 (the second pass): rows carry their hash and value.  The same kernel
+// is the shared-memory path's first pass with logS = logB2 = log2(B) (one
+// partition: the whole side, its buckets the sub-buckets): MODE 1 reads build
+// rows (key, group) and carries (mix64(key), group); MODE 2 reads probe rows
+// (fk, price, disc) and carries (mix64(fk), price * (scale - disc)), or
+// price when disc is null.
+template <typename V, int MODE>
+__global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(const long long* __restrict__ key_in,
+                                                       const V* __restrict__ val_in,
+                                                       const long long* __restrict__ disc_in,
+                                                       long long scale, long long n,
                                                        int logS, int logB2,
                                                        unsigned long long* __restrict__ cursor,
                                                        long long* __restrict__ key_out,
@@ -905,9 +932,9 @@ __global__ void __launch_bounds__(P2T, 2) k_p2_scatter(const long long* __restri
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int nb2 = 1 << logB2;
   const long long ntiles = (n + P2TILE - 1) / P2TILE;
-  const int b0 = 2 * tid, b1 = 2 * tid + 1;  // the sub-buckets this thread scans
-  S.cnt[b0] = 0;
-  S.cnt[b1] = 0;
+  const int bt = P2BPT * tid;  // the first of the sub-buckets this thread scans
+#pragma unroll
+  for (int j = 0; j < P2BPT; ++j) S.cnt[bt + j] = 0;
   long long k[P2I];
   V v[P2I];
   long long tile = blockIdx.x;
@@ -917,7 +944,12 @@ __global__ void __launch_bounds__(P2T, 2) k_p2_scatter(const long long* __restri
       const long long i = t * P2TILE + q * P2T + tid;
       if (i < n) {
         k[q] = stream_ld(key_in + i);
-        v[q] = stream_ld(val_in + i);
+        if (MODE == 2 && disc_in) {
+          v[q] = (V)(long long)((unsigned long long)stream_ld(val_in + i) *
+                                (unsigned long long)(scale - stream_ld(disc_in + i)));
+        } else {
+          v[q] = stream_ld(val_in + i);
+        }
       }
     }
   };
@@ -925,8 +957,13 @@ __global__ void __launch_bounds__(P2T, 2) k_p2_scatter(const long long* __restri
   __syncthreads();
   for (; tile < ntiles; tile += gridDim.x) {
     const long long t0 = tile * P2TILE;
+    if (MODE != 0) {
+#pragma unroll
+      for (int q = 0; q < P2I; ++q) k[q] = (long long)mix64((uint64_t)k[q]);
+    }
     const long long base =
-        ((long long)bucket_of_hash((uint64_t)key_in[t0], logS) >> logB2) << logB2;
+        MODE != 0 ? 0
+                  : ((long long)bucket_of_hash((uint64_t)key_in[t0], logS) >> logB2) << logB2;
     int slot[P2I];  // rank << P2MAXLOG | sub-bucket, or -1
 #pragma unroll
     for (int q = 0; q < P2I; ++q) {
@@ -945,16 +982,21 @@ __global__ void __launch_bounds__(P2T, 2) k_p2_scatter(const long long* __restri
       }
     }
     __syncthreads();
-    const int c0 = S.cnt[b0], c1 = S.cnt[b1];
-    const int s2 = c0 + c1;
+    int cb[P2BPT];
+    int s2 = 0;
+#pragma unroll
+    for (int j = 0; j < P2BPT; ++j) {
+      cb[j] = S.cnt[bt + j];
+      s2 += cb[j];
+    }
     int incl = s2;
     for (int o = 1; o < 32; o <<= 1) {
       const int y = __shfl_up_sync(FULL, incl, o);
       if (lane >= o) incl += y;
     }
     if (lane == 31) S.wsum[w] = incl;
-    S.cnt[b0] = 0;
-    S.cnt[b1] = 0;
+#pragma unroll
+    for (int j = 0; j < P2BPT; ++j) S.cnt[bt + j] = 0;
     __syncthreads();
     int pre = 0, total = 0;
 #pragma unroll
@@ -963,13 +1005,20 @@ __global__ void __launch_bounds__(P2T, 2) k_p2_scatter(const long long* __restri
       pre += q < w ? x : 0;
       total += x;
     }
-    const int ex = pre + incl - s2;
-    S.lofs[b0] = ex;
-    S.lofs[b1] = ex + c0;
+    {
+      int run = pre + incl - s2;
+#pragma unroll
+      for (int j = 0; j < P2BPT; ++j) {
+        S.lofs[bt + j] = run;
+        run += cb[j];
+      }
+    }
     __syncthreads();
     // the claims travel while the tile is placed
-    const long long g0 = c0 ? (long long)atomicAdd(&cursor[base + b0], (unsigned long long)c0) : 0;
-    const long long g1 = c1 ? (long long)atomicAdd(&cursor[base + b1], (unsigned long long)c1) : 0;
+    long long gp[P2BPT];
+#pragma unroll
+    for (int j = 0; j < P2BPT; ++j)
+      gp[j] = cb[j] ? (long long)atomicAdd(&cursor[base + bt + j], (unsigned long long)cb[j]) : 0;
 #pragma unroll
     for (int q = 0; q < P2I; ++q) {
       if (slot[q] < 0) continue;
@@ -977,8 +1026,8 @@ __global__ void __launch_bounds__(P2T, 2) k_p2_scatter(const long long* __restri
       S.sk[e] = k[q];
       S.sv[e] = v[q];
     }
-    S.gpos[b0] = g0;
-    S.gpos[b1] = g1;
+#pragma unroll
+    for (int j = 0; j < P2BPT; ++j) S.gpos[bt + j] = gp[j];
     __syncthreads();
     if (tile + gridDim.x < ntiles) load(tile + gridDim.x);
     for (int e = tid; e < total; e += P2T) {
@@ -1099,6 +1148,25 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
     S.cnt[t] = 0;
   }
   unsigned long long matched = 0, bad_group = 0;
+#if PF_SJ_STATIC
+  // Sub-partitions in turn (block i takes i, i + grid, ...): threads 0-3
+  // load the next one's ranges while the block works on the current one and
+  // store them when it is done.
+  if (tid < 4) {
+    const long long n = blockIdx.x;
+    S.item = n;
+    if (n < a.S) S.bnd[tid] = (long long)(tid < 2 ? a.bstart : a.pstart)[n + (tid & 1)];
+  }
+  __syncthreads();
+  while (true) {
+    const long long s = S.item;
+    const long long b0 = S.bnd[0], b1 = S.bnd[1], p0 = S.bnd[2], p1 = S.bnd[3];
+    __syncthreads();
+    if (s >= a.S) break;
+    const long long nx = s + gridDim.x;
+    long long nb_ = 0;
+    if (tid < 4 && nx < a.S) nb_ = (long long)(tid < 2 ? a.bstart : a.pstart)[nx + (tid & 1)];
+#else
   // thread 0 fetches the next sub-partition and its ranges while the block
   // works on the current one
   auto fetch = [&]() {
@@ -1120,6 +1188,8 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
     if (s >= a.S) break;
     if (tid == 0) fetch();
     if (b1 == b0 || p1 == p0) continue;
+#endif
+    if (b1 > b0 && p1 > p0)
     for (long long c0 = b0; c0 < b1; c0 += SJ_CAP) {
       const int nb = (int)min((long long)SJ_CAP, b1 - c0);
       if (tid == 0) {
@@ -1204,6 +1274,13 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
       }
       __syncthreads();
     }
+#if PF_SJ_STATIC
+    if (tid < 4) {
+      S.bnd[tid] = nb_;
+      if (tid == 0) S.item = nx;
+    }
+    __syncthreads();
+#endif
   }
   for (int o = 16; o; o >>= 1) matched += __shfl_xor_sync(FULL, matched, o);
   if ((tid & 31) == 0 && matched) atomicAdd(&a.stats[0], matched);
@@ -1225,6 +1302,11 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
 // against all of its probe rows.
 #ifndef PF_SJ_STAGED
 #define PF_SJ_STAGED 0
+#endif
+// 1: the shared-memory path's first pass through the tile scatter when
+// B <= P2BINS (PF_FIRST_TILE=0|1 chooses at run time)
+#ifndef PF_FIRST_TILE
+#define PF_FIRST_TILE 1
 #endif
 constexpr int SJST = 1024;
 constexpr int SJ_PIECE = 2048;
@@ -1657,6 +1739,7 @@ struct JaLayout {
   int* pseg2[2];               // [B + 1]: each partition's first segment
   int* hist2[2];               // [segments][2^logB2]
   unsigned long long* cur2;    // [2][s_max]: the pass-2 scatter's cursors
+  unsigned long long* cur1;    // [2B]: the tile scatter's cursors in the first pass
   long long* tot2;             // [2][s_max]: rows per sub-partition
   unsigned long long* start2;  // [2][s_max + 1]
   long long* scan2;            // scan scratch
@@ -1707,6 +1790,7 @@ JaLayout ja_layout(Arena& a, long long nb, long long np, int B, long long n_grou
     }
     l.tot2 = a.take<long long>(2 * (size_t)l.s_max);
     l.cur2 = a.take<unsigned long long>(2 * (size_t)l.s_max);
+    l.cur1 = a.take<unsigned long long>(2 * (size_t)B);
     l.start2 = a.take<unsigned long long>(2 * ((size_t)l.s_max + 1));
     l.scan2 = a.take<long long>(scan_scratch_elems(l.s_max));
     l.sj_counter = a.take<unsigned long long>(1);
@@ -1784,6 +1868,41 @@ int fscatter_both(bool tma, const int64_t* build_key, const int32_t* build_group
   return ok();
 }
 
+// The shared-memory path's first pass through the tile scatter (B <= P2BINS):
+// cursors from the bucket starts, each side's rows hashed and carried with
+// their value.
+int first_pass_tile(const int64_t* build_key, const int32_t* build_group, long long n_build,
+                    const int64_t* probe_fk, const int64_t* probe_price, const int64_t* probe_disc,
+                    long long scale, long long n_probe, int logB, int B, const JaLayout& l,
+                    cudaStream_t st) {
+  PF_CUDA(cudaMemcpyAsync(l.cur1, l.start, 2 * (size_t)B * sizeof(long long),
+                          cudaMemcpyDeviceToDevice, st));
+  const size_t sb = sizeof(P2Smem<int>), sp = sizeof(P2Smem<long long>);
+  if (int rc = opt_in_smem((const void*)k_p2_scatter<int, 1>, sb)) return rc;
+  if (int rc = opt_in_smem((const void*)k_p2_scatter<long long, 2>, sp)) return rc;
+  int ob = 0, op = 0;
+  PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ob, k_p2_scatter<int, 1>, P2T, sb));
+  PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&op, k_p2_scatter<long long, 2>, P2T, sp));
+  const int sms = sm_count();
+  const unsigned gb = (unsigned)std::max<long long>(
+      1, std::min<long long>((n_build + P2TILE - 1) / P2TILE, (long long)std::max(1, ob) * sms));
+  const unsigned gp = (unsigned)std::max<long long>(
+      1, std::min<long long>((n_probe + P2TILE - 1) / P2TILE, (long long)std::max(1, op) * sms));
+  {
+    PF_KERNEL("k_fscatter_build", st);
+    k_p2_scatter<int, 1><<<gb, P2T, sb, st>>>((const long long*)build_key, build_group, nullptr, 0,
+                                              n_build, logB, logB, l.cur1, l.pkey, l.pgrp);
+  }
+  {
+    PF_KERNEL("k_fscatter_probe", st);
+    k_p2_scatter<long long, 2><<<gp, P2T, sp, st>>>(
+        (const long long*)probe_fk, (const long long*)probe_price, (const long long*)probe_disc,
+        scale, n_probe, logB, logB, l.cur1 + B, l.pfk, l.pval);
+  }
+  PF_LAUNCH("k_fscatter");
+  return ok();
+}
+
 // The shared-memory path after the first scatter (counts on the host): the
 // second radix pass into sub-partitions of about SJ_TARGET build rows, the
 // join per sub-partition, the slab split.  Keys are mix64 hashes here.
@@ -1847,19 +1966,19 @@ int join_smem(const JaLayout& l, int B, int logB, const long long* hc, long long
   }
   {
     const size_t sb = sizeof(P2Smem<int>), sp = sizeof(P2Smem<long long>);
-    if (int rc = opt_in_smem((const void*)k_p2_scatter<int>, sb)) return rc;
-    if (int rc = opt_in_smem((const void*)k_p2_scatter<long long>, sp)) return rc;
+    if (int rc = opt_in_smem((const void*)k_p2_scatter<int, 0>, sb)) return rc;
+    if (int rc = opt_in_smem((const void*)k_p2_scatter<long long, 0>, sp)) return rc;
     int ob = 0, op = 0;
-    PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ob, k_p2_scatter<int>, P2T, sb));
-    PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&op, k_p2_scatter<long long>, P2T, sp));
+    PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ob, k_p2_scatter<int, 0>, P2T, sb));
+    PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&op, k_p2_scatter<long long, 0>, P2T, sp));
     const unsigned gb = (unsigned)std::max<long long>(
         1, std::min<long long>((n_build + P2TILE - 1) / P2TILE, (long long)std::max(1, ob) * sms));
     const unsigned gp = (unsigned)std::max<long long>(
         1, std::min<long long>((n_probe + P2TILE - 1) / P2TILE, (long long)std::max(1, op) * sms));
     PF_KERNEL("k_p2_scatter", st);
-    k_p2_scatter<int><<<gb, P2T, sb, st>>>(l.pkey, l.pgrp, n_build, logS, logB2, l.cur2, l.pkey2,
+    k_p2_scatter<int, 0><<<gb, P2T, sb, st>>>(l.pkey, l.pgrp, nullptr, 0, n_build, logS, logB2, l.cur2, l.pkey2,
                                            l.pgrp2);
-    k_p2_scatter<long long><<<gp, P2T, sp, st>>>(l.pfk, l.pval, n_probe, logS, logB2,
+    k_p2_scatter<long long, 0><<<gp, P2T, sp, st>>>(l.pfk, l.pval, nullptr, 0, n_probe, logS, logB2,
                                                  l.cur2 + l.s_max, l.pfk2, l.pval2);
   }
   PF_LAUNCH("k_p2_scatter");
@@ -1999,7 +2118,11 @@ extern "C" int pf_join_aggregate(const int64_t* build_key, const int32_t* build_
                    aligned16(probe_price) && (!probe_disc || aligned16(probe_disc)) &&
                    getenv("PF_NO_TMA") == nullptr;
   const bool smem_path = join_path_smem() != 0;
-  if (int rc = smem_path ? fscatter_both<true>(tma, build_key, build_group, n_build, probe_fk,
+  const char* fe = getenv("PF_FIRST_TILE");
+  const bool tile_first = smem_path && B <= P2BINS && (fe ? fe[0] != '0' : PF_FIRST_TILE);
+  if (int rc = tile_first ? first_pass_tile(build_key, build_group, n_build, probe_fk, probe_price,
+                                            probe_disc, scale, n_probe, logB, B, l, st)
+               : smem_path ? fscatter_both<true>(tma, build_key, build_group, n_build, probe_fk,
                                                 probe_price, probe_disc, scale, n_probe, chunk_b,
                                                 nch_b, chunk_p, nch_p, logB, B, l, stats_out, st)
                          : fscatter_both<false>(tma, build_key, build_group, n_build, probe_fk,
