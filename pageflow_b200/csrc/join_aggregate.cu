@@ -804,12 +804,16 @@ static_assert(P2BINS % P2T == 0 && P2BPT >= 1, "whole sub-buckets a thread in th
 #define PF_SJ_MINB 2
 #endif
 #ifndef PF_SJ_U
-#define PF_SJ_U 4
+#define PF_SJ_U 1
 #endif
 // 1: sub-partitions taken in turn by block index (their ranges loaded one
 // sub-partition ahead), 0: from a shared counter
 #ifndef PF_SJ_STATIC
 #define PF_SJ_STATIC 0
+#endif
+// 1: the probe loop loads the next round's rows before looking up this one's
+#ifndef PF_SJ_PIPE
+#define PF_SJ_PIPE 1
 #endif
 constexpr int SJT = PF_SJT;       // threads of the join
 #ifndef PF_SJ_LOGTS
@@ -1198,6 +1202,16 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
         S.min_cnt = 0;
       }
       __syncthreads();
+#if PF_SJ_PIPE
+      // the first probe round's rows load while the build runs
+      long long key[SJ_U], val[SJ_U];
+#pragma unroll
+      for (int u = 0; u < SJ_U; ++u) {
+        const long long i = p0 + u * SJT + tid;
+        key[u] = i < p1 ? stream_ld(a.pfk + i) : 0;
+        val[u] = i < p1 ? stream_ld(a.pval + i) : 0;
+      }
+#endif
       // build: each build row a slot of its own (all of a thread's rows
       // loaded first)
       long long bk[SJ_BU];
@@ -1238,7 +1252,30 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
         S.slot_of[u * SJT + tid] = (unsigned short)t;
       }
       __syncthreads();
-      // probe, SJ_U rows a thread in flight
+      // probe, SJ_U rows a thread a round
+#if PF_SJ_PIPE
+      // the next round's rows load while this round's are looked up
+      {
+        long long nkey[SJ_U], nval[SJ_U];
+        for (long long i0 = p0; i0 < p1; i0 += (long long)SJT * SJ_U) {
+          const long long n0 = i0 + (long long)SJT * SJ_U;
+#pragma unroll
+          for (int u = 0; u < SJ_U; ++u) {
+            const long long i = n0 + u * SJT + tid;
+            nkey[u] = i < p1 ? stream_ld(a.pfk + i) : 0;
+            nval[u] = i < p1 ? stream_ld(a.pval + i) : 0;
+          }
+#pragma unroll
+          for (int u = 0; u < SJ_U; ++u)
+            if (i0 + u * SJT + tid < p1) sj_probe(S, key[u], val[u], a.logS, matched);
+#pragma unroll
+          for (int u = 0; u < SJ_U; ++u) {
+            key[u] = nkey[u];
+            val[u] = nval[u];
+          }
+        }
+      }
+#else
       for (long long i0 = p0; i0 < p1; i0 += (long long)SJT * SJ_U) {
         long long key[SJ_U], val[SJ_U];
 #pragma unroll
@@ -1253,6 +1290,7 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
         for (int u = 0; u < SJ_U; ++u)
           if (i0 + u * SJT + tid < p1) sj_probe(S, key[u], val[u], a.logS, matched);
       }
+#endif
       __syncthreads();
       // flush every build row that matched, and empty its slot
       for (int j = tid; j < nb; j += SJT) {
