@@ -894,10 +894,16 @@ __global__ void k_p2_colsum(const int* __restrict__ hist, const int* __restrict_
   tot[idx] = run;
 }
 
+// A staged row: key and value in one 16-byte record (one shared-memory store
+// to place it, one load to write it out).
+struct alignas(16) P2Row {
+  long long k;
+  long long v;
+};
+
 template <typename V>
 struct P2Smem {
-  long long sk[P2TILE];
-  V sv[P2TILE];
+  P2Row sr[P2TILE];
   int cnt[P2BINS];         // rows of a sub-bucket in the tile, then zero again
   int lofs[P2BINS];        // a sub-bucket's first place in the tile
   long long gpos[P2BINS];  // the sub-bucket's claimed first place in the output
@@ -942,18 +948,17 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(const long long*
   long long k[P2I];
   V v[P2I];
   long long tile = blockIdx.x;
+  // MODE 2 with a discount: the raw price in v and the discount in dv until
+  // the tile's turn comes, so the prefetch never waits for its loads
+  long long dv[MODE == 2 ? P2I : 1];
   auto load = [&](long long t) {
 #pragma unroll
     for (int q = 0; q < P2I; ++q) {
       const long long i = t * P2TILE + q * P2T + tid;
       if (i < n) {
         k[q] = stream_ld(key_in + i);
-        if (MODE == 2 && disc_in) {
-          v[q] = (V)(long long)((unsigned long long)stream_ld(val_in + i) *
-                                (unsigned long long)(scale - stream_ld(disc_in + i)));
-        } else {
-          v[q] = stream_ld(val_in + i);
-        }
+        v[q] = stream_ld(val_in + i);
+        if (MODE == 2 && disc_in) dv[q] = stream_ld(disc_in + i);
       }
     }
   };
@@ -964,6 +969,11 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(const long long*
     if (MODE != 0) {
 #pragma unroll
       for (int q = 0; q < P2I; ++q) k[q] = (long long)mix64((uint64_t)k[q]);
+    }
+    if (MODE == 2 && disc_in) {
+#pragma unroll
+      for (int q = 0; q < P2I; ++q)
+        v[q] = (V)(long long)((unsigned long long)v[q] * (unsigned long long)(scale - dv[q]));
     }
     const long long base =
         MODE != 0 ? 0
@@ -1027,19 +1037,18 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(const long long*
     for (int q = 0; q < P2I; ++q) {
       if (slot[q] < 0) continue;
       const int e = S.lofs[slot[q] & (P2BINS - 1)] + (slot[q] >> P2MAXLOG);
-      S.sk[e] = k[q];
-      S.sv[e] = v[q];
+      S.sr[e] = P2Row{k[q], (long long)v[q]};
     }
 #pragma unroll
     for (int j = 0; j < P2BPT; ++j) S.gpos[bt + j] = gp[j];
     __syncthreads();
     if (tile + gridDim.x < ntiles) load(tile + gridDim.x);
     for (int e = tid; e < total; e += P2T) {
-      const long long key = S.sk[e];
-      const int b = (int)(bucket_of_hash((uint64_t)key, logS) - base);
+      const P2Row r = S.sr[e];
+      const int b = (int)(bucket_of_hash((uint64_t)r.k, logS) - base);
       const long long pos = S.gpos[b] + (e - S.lofs[b]);
-      key_out[pos] = key;
-      val_out[pos] = S.sv[e];
+      key_out[pos] = r.k;
+      val_out[pos] = (V)r.v;
     }
     __syncthreads();
   }
