@@ -806,11 +806,6 @@ static_assert(P2BINS % P2T == 0 && P2BPT >= 1, "whole sub-buckets a thread in th
 #ifndef PF_SJ_U
 #define PF_SJ_U 1
 #endif
-// 1: sub-partitions taken in turn by block index (their ranges loaded one
-// sub-partition ahead), 0: from a shared counter
-#ifndef PF_SJ_STATIC
-#define PF_SJ_STATIC 0
-#endif
 // 1: the probe loop loads the next round's rows before looking up this one's
 #ifndef PF_SJ_PIPE
 #define PF_SJ_PIPE 1
@@ -1087,7 +1082,8 @@ __device__ __forceinline__ void sj_sum_add(SJSum& c, long long val) {
   const unsigned l = (unsigned)(unsigned long long)val;
   const unsigned h = (unsigned)((unsigned long long)val >> 32);
   const unsigned old = atomicAdd(&c.lo, l);
-  atomicAdd(&c.hi, h + (old + l < old ? 1u : 0u));
+  const unsigned hc = h + (old + l < old ? 1u : 0u);
+  if (hc) atomicAdd(&c.hi, hc);  // zero for a value below 2^32 without a carry
 #else
   atomicAdd(&c.v, (unsigned long long)val);
 #endif
@@ -1117,8 +1113,8 @@ struct SJSmem {
   long long min_sum;               // the key hashing to INT64_MIN, kept apart
   unsigned min_cnt, min_goff;
   int has_min;
-  long long item;                  // the next sub-partition and its row ranges
-  long long bnd[4];
+  long long item[2];               // sub-partition and its row ranges, double-buffered
+  long long bnd[2][4];
 };
 
 __device__ __forceinline__ unsigned sj_slot(uint64_t h, int logS) {
@@ -1161,56 +1157,38 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
     S.cnt[t] = 0;
   }
   unsigned long long matched = 0, bad_group = 0;
-#if PF_SJ_STATIC
-  // Sub-partitions in turn (block i takes i, i + grid, ...): threads 0-3
-  // load the next one's ranges while the block works on the current one and
-  // store them when it is done.
-  if (tid < 4) {
-    const long long n = blockIdx.x;
-    S.item = n;
-    if (n < a.S) S.bnd[tid] = (long long)(tid < 2 ? a.bstart : a.pstart)[n + (tid & 1)];
-  }
-  __syncthreads();
-  while (true) {
-    const long long s = S.item;
-    const long long b0 = S.bnd[0], b1 = S.bnd[1], p0 = S.bnd[2], p1 = S.bnd[3];
-    __syncthreads();
-    if (s >= a.S) break;
-    const long long nx = s + gridDim.x;
-    long long nb_ = 0;
-    if (tid < 4 && nx < a.S) nb_ = (long long)(tid < 2 ? a.bstart : a.pstart)[nx + (tid & 1)];
-#else
-  // thread 0 fetches the next sub-partition and its ranges while the block
-  // works on the current one
-  auto fetch = [&]() {
+  // Thread 0 fetches the next sub-partition and its ranges into the other
+  // half of a double-buffered descriptor while the block works on the
+  // current one; the barriers of the work make it visible.
+  auto fetch = [&](int slot) {
     const long long n = (long long)atomicAdd(a.counter, 1ULL);
-    S.item = n;
+    S.item[slot] = n;
     if (n < a.S) {
-      S.bnd[0] = (long long)a.bstart[n];
-      S.bnd[1] = (long long)a.bstart[n + 1];
-      S.bnd[2] = (long long)a.pstart[n];
-      S.bnd[3] = (long long)a.pstart[n + 1];
+      S.bnd[slot][0] = (long long)a.bstart[n];
+      S.bnd[slot][1] = (long long)a.bstart[n + 1];
+      S.bnd[slot][2] = (long long)a.pstart[n];
+      S.bnd[slot][3] = (long long)a.pstart[n + 1];
     }
   };
-  if (tid == 0) fetch();
-  while (true) {
-    __syncthreads();
-    const long long s = S.item;
-    const long long b0 = S.bnd[0], b1 = S.bnd[1], p0 = S.bnd[2], p1 = S.bnd[3];
-    __syncthreads();
+  if (tid == 0) {
+    S.has_min = 0;
+    S.min_sum = 0;
+    S.min_cnt = 0;
+    fetch(0);
+  }
+  __syncthreads();
+  for (int cur = 0;; cur ^= 1) {
+    const long long s = S.item[cur];
+    const long long b0 = S.bnd[cur][0], b1 = S.bnd[cur][1];
+    const long long p0 = S.bnd[cur][2], p1 = S.bnd[cur][3];
     if (s >= a.S) break;
-    if (tid == 0) fetch();
-    if (b1 == b0 || p1 == p0) continue;
-#endif
-    if (b1 > b0 && p1 > p0)
+    if (tid == 0) fetch(cur ^ 1);
+    if (b1 == b0 || p1 == p0) {
+      __syncthreads();
+      continue;
+    }
     for (long long c0 = b0; c0 < b1; c0 += SJ_CAP) {
       const int nb = (int)min((long long)SJ_CAP, b1 - c0);
-      if (tid == 0) {
-        S.has_min = 0;
-        S.min_sum = 0;
-        S.min_cnt = 0;
-      }
-      __syncthreads();
 #if PF_SJ_PIPE
       // the first probe round's rows load while the build runs
       long long key[SJ_U], val[SJ_U];
@@ -1315,19 +1293,18 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
         sj_sum_clear(S.sum[t]);
         S.cnt[t] = 0;
       }
-      if (tid == 0 && S.has_min && S.min_cnt && S.min_goff != SJ_NONE) {
-        atomicAdd(&a.slab[2 * (unsigned long long)S.min_goff], (unsigned long long)S.min_sum);
-        atomicAdd(&a.slab[2 * (unsigned long long)S.min_goff + 1], (unsigned long long)S.min_cnt);
+      if (tid == 0) {
+        if (S.has_min && S.min_cnt && S.min_goff != SJ_NONE) {
+          atomicAdd(&a.slab[2 * (unsigned long long)S.min_goff], (unsigned long long)S.min_sum);
+          atomicAdd(&a.slab[2 * (unsigned long long)S.min_goff + 1],
+                    (unsigned long long)S.min_cnt);
+        }
+        S.has_min = 0;
+        S.min_sum = 0;
+        S.min_cnt = 0;
       }
       __syncthreads();
     }
-#if PF_SJ_STATIC
-    if (tid < 4) {
-      S.bnd[tid] = nb_;
-      if (tid == 0) S.item = nx;
-    }
-    __syncthreads();
-#endif
   }
   for (int o = 16; o; o >>= 1) matched += __shfl_xor_sync(FULL, matched, o);
   if ((tid & 31) == 0 && matched) atomicAdd(&a.stats[0], matched);
