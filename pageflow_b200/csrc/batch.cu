@@ -31,6 +31,11 @@ constexpr int BT2 = 256;
 #ifndef PF_BATCH_BV
 #define PF_BATCH_BV 1
 #endif
+// 1: the probe loop loads the next round's keys and values while this round
+// probes its slots
+#ifndef PF_BATCH_PIPE
+#define PF_BATCH_PIPE 1
+#endif
 constexpr int BV = PF_BATCH_BV;  // rows a thread keeps in flight
 // 1: a probe item adds into the block's group cache (agg.cuh) and flushes it
 // at the item's end, so the hot groups of a skewed instance cost one global
@@ -260,12 +265,43 @@ __global__ void __launch_bounds__(BT2) k_batch(Header* h, const Desc* d, const i
       // BV rows a thread at a time: keys, then every first slot and value,
       // then the (rare) collisions
       const long long lo = (local - D.nbi) * PITEM, hi = min(D.np, lo + PITEM);
+#if PF_BATCH_PIPE
+      // the next round's keys and values load while this round probes
+      unsigned long long key[BV];
+      long long value[BV];
+#pragma unroll
+      for (int k = 0; k < BV; ++k) {
+        const long long i = lo + k * BT2 + threadIdx.x;
+        const bool l = i < hi && D.tcap > 0;
+        key[k] = l ? (unsigned long long)D.pfk[i] : 0ULL;
+        value[k] = l ? D.pval[i] : 0;
+      }
+#endif
       for (long long i0 = lo; i0 < hi; i0 += BT2 * BV) {
-        unsigned long long key[BV];
         unsigned pos[BV];
         ulonglong2 sl[BV];
-        long long value[BV], g[BV];
+        long long g[BV];
         bool live[BV];
+#if PF_BATCH_PIPE
+        unsigned long long nkey[BV];
+        long long nval[BV];
+#pragma unroll
+        for (int k = 0; k < BV; ++k) {
+          const long long i = i0 + (long long)BT2 * BV + k * BT2 + threadIdx.x;
+          const bool l = i < hi && D.tcap > 0;
+          nkey[k] = l ? (unsigned long long)D.pfk[i] : 0ULL;
+          nval[k] = l ? D.pval[i] : 0;
+        }
+#pragma unroll
+        for (int k = 0; k < BV; ++k) {
+          live[k] = i0 + k * BT2 + threadIdx.x < hi && D.tcap > 0;
+          pos[k] = live[k] ? first_slot(mix64(key[k]), D.tcap) : 0u;
+          sl[k] = live[k] ? __ldcg(reinterpret_cast<const ulonglong2*>(tables + D.toff + pos[k]))
+                          : make_ulonglong2(0ULL, 0ULL);
+        }
+#else
+        unsigned long long key[BV];
+        long long value[BV];
 #pragma unroll
         for (int k = 0; k < BV; ++k) {
           const long long i = i0 + k * BT2 + threadIdx.x;
@@ -280,6 +316,7 @@ __global__ void __launch_bounds__(BT2) k_batch(Header* h, const Desc* d, const i
                           : make_ulonglong2(0ULL, 0ULL);
           value[k] = live[k] ? D.pval[i] : 0;
         }
+#endif
 #pragma unroll
         for (int k = 0; k < BV; ++k) {
           g[k] = -1;
@@ -308,6 +345,13 @@ __global__ void __launch_bounds__(BT2) k_batch(Header* h, const Desc* d, const i
           combined_add(slabs + 2 * D.soff, g[k], g[k] >= 0 ? value[k] : 0);
 #endif
         }
+#if PF_BATCH_PIPE
+#pragma unroll
+        for (int k = 0; k < BV; ++k) {
+          key[k] = nkey[k];
+          value[k] = nval[k];
+        }
+#endif
       }
 #if PF_BATCH_CACHE
       cache_flush(gc, slabs + 2 * D.soff);

@@ -815,8 +815,14 @@ constexpr int SJT = PF_SJT;       // threads of the join
 #define PF_SJ_LOGTS 12
 #endif
 constexpr int SJ_TS = 1 << PF_SJ_LOGTS;        // table slots
-constexpr int SJ_CAP = SJ_TS / 2;              // build rows a table takes
-constexpr long long SJ_TARGET = SJ_TS / 3;     // build rows a sub-partition aims at
+#ifndef PF_SJ_CAP
+#define PF_SJ_CAP (SJ_TS / 2)
+#endif
+#ifndef PF_SJ_TARGET
+#define PF_SJ_TARGET (SJ_TS / 3)
+#endif
+constexpr int SJ_CAP = PF_SJ_CAP;              // build rows a table takes
+constexpr long long SJ_TARGET = PF_SJ_TARGET;  // build rows a sub-partition aims at
 constexpr long long SJ_EMPTY = LLONG_MIN;
 constexpr unsigned SJ_NONE = 0xffffffffu;
 constexpr int SJ_U = PF_SJ_U;                  // probe rows a thread holds at once
