@@ -37,6 +37,10 @@ constexpr int ST = 256;
 #ifndef PF_SERVE_SV
 #define PF_SERVE_SV 4
 #endif
+// 1: the probe loop loads the next round's dates while this round runs
+#ifndef PF_SERVE_PIPE
+#define PF_SERVE_PIPE 1
+#endif
 constexpr int SV = PF_SERVE_SV;  // probe rows a thread keeps in flight
 // 1: probe items add through the block's group cache (agg.cuh), flushed at
 // the item's end; 0: hot_add into the slab directly.
@@ -204,17 +208,36 @@ __global__ void __launch_bounds__(ST) k_serve(SHead* h, const SReq* __restrict__
       // thread keeps SV independent loads in flight
       const long long lo = R.r0 + local * PROBE_ROWS, hi = min(R.r1, lo + PROBE_ROWS);
       const unsigned long long mask = (1ULL << R.logcap) - 1;
+#if PF_SERVE_PIPE
+      // the next round's dates load while this round runs
+      int dt[SV];
+#pragma unroll
+      for (int k = 0; k < SV; ++k) {
+        const long long i = lo + k * ST + threadIdx.x;
+        dt[k] = i < hi ? R.date[i] : INT_MIN;
+      }
+#endif
       for (long long i0 = lo; i0 < hi; i0 += ST * SV) {
         bool keep[SV];
         unsigned long long key[SV], slot[SV];
         ulonglong2 sl[SV];
         long long g[SV], value[SV];
+#if PF_SERVE_PIPE
+#pragma unroll
+        for (int k = 0; k < SV; ++k) keep[k] = dt[k] >= R.lo && dt[k] < R.hi;
+#pragma unroll
+        for (int k = 0; k < SV; ++k) {
+          const long long i = i0 + (long long)ST * SV + k * ST + threadIdx.x;
+          dt[k] = i < hi ? R.date[i] : INT_MIN;
+        }
+#else
 #pragma unroll
         for (int k = 0; k < SV; ++k) {
           const long long i = i0 + k * ST + threadIdx.x;
           const int d = i < hi ? R.date[i] : INT_MIN;
           keep[k] = d >= R.lo && d < R.hi;
         }
+#endif
 #pragma unroll
         for (int k = 0; k < SV; ++k) {
           const long long i = i0 + k * ST + threadIdx.x;

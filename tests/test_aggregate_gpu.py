@@ -286,3 +286,26 @@ def test_extreme_keys_join(join_path):
         plan = JoinAggregate(7, 11, 0, 7, "cuda", B=B)
         _assert_groups(plan.run(bkey, bgrp, fk, price, disc), want)
         assert plan.read_stats().matched == want[3] == 9
+
+
+@pytest.mark.parametrize("B", [1, 64])
+def test_skewed_probe_keys(B, join_path):
+    """Zipf-like probe keys: a few build keys take most probe rows, so their
+    sub-partitions hold far more probe rows than the rest and their table
+    cells (or L2 slots) take most of the adds."""
+    g = torch.Generator().manual_seed(21)
+    nb, np_ = 200_000, 2_000_000
+    bkey = torch.randperm(4 * nb, generator=g)[:nb].to(torch.int64) * 104729 - (1 << 40)
+    bgrp = torch.randint(0, 5_000, (nb,), generator=g, dtype=torch.int32)
+    ranks = torch.rand(np_, generator=g).pow(6).mul(nb).to(torch.int64).clamp_(max=nb - 1)
+    fk = bkey[ranks]
+    fk[::13] += 1                                     # some rows match nothing
+    price = torch.randint(-(1 << 28), 1 << 28, (np_,), generator=g)
+    disc = torch.randint(0, 11, (np_,), generator=g)
+    args = [t.cuda() for t in (bkey, bgrp, fk, price, disc)]
+    want = _oracle_groups(*args, 0, 5_000)
+    plan = JoinAggregate(nb, np_, 0, 5_000, "cuda", B=B)
+    _assert_groups(plan.run(*args), want)
+    assert plan.read_stats().matched == want[3]
+    top = torch.bincount(ranks, minlength=nb).max().item()
+    assert top > np_ // 50                            # the hottest key takes > 2% of the rows
