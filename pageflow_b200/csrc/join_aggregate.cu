@@ -1123,14 +1123,18 @@ struct SJSmem {
   long long bnd[2][4];
 };
 
+// A row's home slot: the PF_SJ_LOGTS hash bits after the top logS ones (which
+// all rows of a sub-partition share); from the high word alone when they lie
+// in it.
 __device__ __forceinline__ unsigned sj_slot(uint64_t h, int logS) {
+  if (logS + PF_SJ_LOGTS <= 32) return ((unsigned)(h >> 32) << logS) >> (32 - PF_SJ_LOGTS);
   return (unsigned)((h << logS) >> (64 - PF_SJ_LOGTS));
 }
 
 // One probe row against the chunk's table: its value and 1 into the cell of
 // the build row with its key.
 __device__ __forceinline__ void sj_probe(SJSmem& S, long long key, long long val, int logS,
-                                         unsigned long long& matched) {
+                                         unsigned& matched) {
   if (key == SJ_EMPTY) {
     if (S.has_min) {
       atomicAdd((unsigned long long*)&S.min_sum, (unsigned long long)val);
@@ -1162,7 +1166,8 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
     sj_sum_clear(S.sum[t]);
     S.cnt[t] = 0;
   }
-  unsigned long long matched = 0, bad_group = 0;
+  unsigned matched = 0;  // rows a thread matched (below 2^32: at most 2^40 / SJT)
+  unsigned long long bad_group = 0;
   // Thread 0 fetches the next sub-partition and its ranges into the other
   // half of a double-buffered descriptor while the block works on the
   // current one; the barriers of the work make it visible.
@@ -1196,13 +1201,17 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
     for (long long c0 = b0; c0 < b1; c0 += SJ_CAP) {
       const int nb = (int)min((long long)SJ_CAP, b1 - c0);
 #if PF_SJ_PIPE
-      // the first probe round's rows load while the build runs
+      // the first probe round's rows load while the build runs; pk / pv walk
+      // this thread's rows (every SJT-th from p0 + tid), rem counts the rows
+      // from the current one to the end of the range
+      const long long* pk = a.pfk + p0 + tid;
+      const long long* pv = a.pval + p0 + tid;
+      const long long rem = p1 - p0 - tid;
       long long key[SJ_U], val[SJ_U];
 #pragma unroll
       for (int u = 0; u < SJ_U; ++u) {
-        const long long i = p0 + u * SJT + tid;
-        key[u] = i < p1 ? stream_ld(a.pfk + i) : 0;
-        val[u] = i < p1 ? stream_ld(a.pval + i) : 0;
+        key[u] = u * SJT < rem ? stream_ld(pk + u * SJT) : 0;
+        val[u] = u * SJT < rem ? stream_ld(pv + u * SJT) : 0;
       }
 #endif
       // build: each build row a slot of its own (all of a thread's rows
@@ -1250,17 +1259,19 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
       // the next round's rows load while this round's are looked up
       {
         long long nkey[SJ_U], nval[SJ_U];
-        for (long long i0 = p0; i0 < p1; i0 += (long long)SJT * SJ_U) {
-          const long long n0 = i0 + (long long)SJT * SJ_U;
+        constexpr int STEP = SJT * SJ_U;
+        for (long long r = rem; r > 0; r -= STEP) {
+          pk += STEP;
+          pv += STEP;
+          const long long rn = r - STEP;
 #pragma unroll
           for (int u = 0; u < SJ_U; ++u) {
-            const long long i = n0 + u * SJT + tid;
-            nkey[u] = i < p1 ? stream_ld(a.pfk + i) : 0;
-            nval[u] = i < p1 ? stream_ld(a.pval + i) : 0;
+            nkey[u] = u * SJT < rn ? stream_ld(pk + u * SJT) : 0;
+            nval[u] = u * SJT < rn ? stream_ld(pv + u * SJT) : 0;
           }
 #pragma unroll
           for (int u = 0; u < SJ_U; ++u)
-            if (i0 + u * SJT + tid < p1) sj_probe(S, key[u], val[u], a.logS, matched);
+            if (u * SJT < r) sj_probe(S, key[u], val[u], a.logS, matched);
 #pragma unroll
           for (int u = 0; u < SJ_U; ++u) {
             key[u] = nkey[u];
@@ -1312,8 +1323,9 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
       __syncthreads();
     }
   }
-  for (int o = 16; o; o >>= 1) matched += __shfl_xor_sync(FULL, matched, o);
-  if ((tid & 31) == 0 && matched) atomicAdd(&a.stats[0], matched);
+  unsigned long long m = matched;
+  for (int o = 16; o; o >>= 1) m += __shfl_xor_sync(FULL, m, o);
+  if ((tid & 31) == 0 && m) atomicAdd(&a.stats[0], m);
   if (bad_group) atomicAdd(&a.stats[2], bad_group);
 }
 
