@@ -793,6 +793,14 @@ __global__ void __launch_bounds__(PT2, PF_PROBE_MINB) k_fround(RoundArgs pa, Rou
 constexpr int P2T = PF_P2T;
 constexpr int P2I = PF_P2I;
 constexpr int P2TILE = P2T * P2I;  // rows a pass-2 tile
+// The first pass's probe side carries three input columns a row into its
+// registers: 6 rows a thread (6144-row tiles) keep it within 64 registers
+// without spilling (measured against 8 rows, which spilled: 5.50 vs 5.86 ms
+// on 600M probe rows).
+#ifndef PF_P2_RI2
+#define PF_P2_RI2 6
+#endif
+constexpr int P2RI2 = PF_P2_RI2;
 constexpr int P2MAXLOG = 10;       // sub-buckets a partition splits into, log2, at most
 constexpr int P2BINS = 1 << P2MAXLOG;
 constexpr int P2BPT = P2BINS / P2T;  // sub-buckets a thread scans
@@ -929,7 +937,8 @@ struct P2Smem {
 // rows (key, group) and carries (mix64(key), group); MODE 2 reads probe rows
 // (fk, price, disc) and carries (mix64(fk), price * (scale - disc)), or
 // price when disc is null.
-template <typename V, int MODE>
+// RI rows a thread a tile (a tile of P2T * RI <= P2TILE rows).
+template <typename V, int MODE, int RI = P2I>
 __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(const long long* __restrict__ key_in,
                                                        const V* __restrict__ val_in,
                                                        const long long* __restrict__ disc_in,
@@ -942,20 +951,22 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(const long long*
   P2Smem<V>& S = *reinterpret_cast<P2Smem<V>*>(p2_smem);
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int nb2 = 1 << logB2;
-  const long long ntiles = (n + P2TILE - 1) / P2TILE;
+  static_assert(P2T * RI <= P2TILE, "a tile fits the staging");
+  constexpr int TILE = P2T * RI;
+  const long long ntiles = (n + TILE - 1) / TILE;
   const int bt = P2BPT * tid;  // the first of the sub-buckets this thread scans
 #pragma unroll
   for (int j = 0; j < P2BPT; ++j) S.cnt[bt + j] = 0;
-  long long k[P2I];
-  V v[P2I];
+  long long k[RI];
+  V v[RI];
   long long tile = blockIdx.x;
   // MODE 2 with a discount: the raw price in v and the discount in dv until
   // the tile's turn comes, so the prefetch never waits for its loads
-  long long dv[MODE == 2 ? P2I : 1];
+  long long dv[MODE == 2 ? RI : 1];
   auto load = [&](long long t) {
 #pragma unroll
-    for (int q = 0; q < P2I; ++q) {
-      const long long i = t * P2TILE + q * P2T + tid;
+    for (int q = 0; q < RI; ++q) {
+      const long long i = t * TILE + q * P2T + tid;
       if (i < n) {
         k[q] = stream_ld(key_in + i);
         v[q] = stream_ld(val_in + i);
@@ -966,22 +977,22 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(const long long*
   if (tile < ntiles) load(tile);
   __syncthreads();
   for (; tile < ntiles; tile += gridDim.x) {
-    const long long t0 = tile * P2TILE;
+    const long long t0 = tile * TILE;
     if (MODE != 0) {
 #pragma unroll
-      for (int q = 0; q < P2I; ++q) k[q] = (long long)mix64((uint64_t)k[q]);
+      for (int q = 0; q < RI; ++q) k[q] = (long long)mix64((uint64_t)k[q]);
     }
     if (MODE == 2 && disc_in) {
 #pragma unroll
-      for (int q = 0; q < P2I; ++q)
+      for (int q = 0; q < RI; ++q)
         v[q] = (V)(long long)((unsigned long long)v[q] * (unsigned long long)(scale - dv[q]));
     }
     const long long base =
         MODE != 0 ? 0
                   : ((long long)bucket_of_hash((uint64_t)key_in[t0], logS) >> logB2) << logB2;
-    int slot[P2I];  // rank << P2MAXLOG | sub-bucket, or -1
+    int slot[RI];  // rank << P2MAXLOG | sub-bucket, or -1
 #pragma unroll
-    for (int q = 0; q < P2I; ++q) {
+    for (int q = 0; q < RI; ++q) {
       const long long i = t0 + q * P2T + tid;
       slot[q] = -1;
       if (i < n) {
@@ -1035,7 +1046,7 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(const long long*
     for (int j = 0; j < P2BPT; ++j)
       gp[j] = cb[j] ? (long long)atomicAdd(&cursor[base + bt + j], (unsigned long long)cb[j]) : 0;
 #pragma unroll
-    for (int q = 0; q < P2I; ++q) {
+    for (int q = 0; q < RI; ++q) {
       if (slot[q] < 0) continue;
       const int e = S.lofs[slot[q] & (P2BINS - 1)] + (slot[q] >> P2MAXLOG);
       S.sr[e] = P2Row{k[q], (long long)v[q]};
@@ -1921,15 +1932,17 @@ int first_pass_tile(const int64_t* build_key, const int32_t* build_group, long l
                           cudaMemcpyDeviceToDevice, st));
   const size_t sb = sizeof(P2Smem<int>), sp = sizeof(P2Smem<long long>);
   if (int rc = opt_in_smem((const void*)k_p2_scatter<int, 1>, sb)) return rc;
-  if (int rc = opt_in_smem((const void*)k_p2_scatter<long long, 2>, sp)) return rc;
+  if (int rc = opt_in_smem((const void*)k_p2_scatter<long long, 2, P2RI2>, sp)) return rc;
   int ob = 0, op = 0;
   PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ob, k_p2_scatter<int, 1>, P2T, sb));
-  PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&op, k_p2_scatter<long long, 2>, P2T, sp));
+  PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&op, k_p2_scatter<long long, 2, P2RI2>,
+                                                        P2T, sp));
   const int sms = sm_count();
   const unsigned gb = (unsigned)std::max<long long>(
       1, std::min<long long>((n_build + P2TILE - 1) / P2TILE, (long long)std::max(1, ob) * sms));
+  constexpr int tile2 = P2T * P2RI2;
   const unsigned gp = (unsigned)std::max<long long>(
-      1, std::min<long long>((n_probe + P2TILE - 1) / P2TILE, (long long)std::max(1, op) * sms));
+      1, std::min<long long>((n_probe + tile2 - 1) / tile2, (long long)std::max(1, op) * sms));
   {
     PF_KERNEL("k_fscatter_build", st);
     k_p2_scatter<int, 1><<<gb, P2T, sb, st>>>((const long long*)build_key, build_group, nullptr, 0,
@@ -1937,7 +1950,7 @@ int first_pass_tile(const int64_t* build_key, const int32_t* build_group, long l
   }
   {
     PF_KERNEL("k_fscatter_probe", st);
-    k_p2_scatter<long long, 2><<<gp, P2T, sp, st>>>(
+    k_p2_scatter<long long, 2, P2RI2><<<gp, P2T, sp, st>>>(
         (const long long*)probe_fk, (const long long*)probe_price, (const long long*)probe_disc,
         scale, n_probe, logB, logB, l.cur1 + B, l.pfk, l.pval);
   }
