@@ -963,7 +963,9 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(const long long*
   // MODE 2 with a discount: the raw price in v and the discount in dv until
   // the tile's turn comes, so the prefetch never waits for its loads
   long long dv[MODE == 2 ? RI : 1];
+  long long k0 = 0;  // MODE 0: the tile's first key (its partition), loaded with the tile
   auto load = [&](long long t) {
+    if (MODE == 0) k0 = key_in[t * TILE];
 #pragma unroll
     for (int q = 0; q < RI; ++q) {
       const long long i = t * TILE + q * P2T + tid;
@@ -988,8 +990,7 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(const long long*
         v[q] = (V)(long long)((unsigned long long)v[q] * (unsigned long long)(scale - dv[q]));
     }
     const long long base =
-        MODE != 0 ? 0
-                  : ((long long)bucket_of_hash((uint64_t)key_in[t0], logS) >> logB2) << logB2;
+        MODE != 0 ? 0 : ((long long)bucket_of_hash((uint64_t)k0, logS) >> logB2) << logB2;
     int slot[RI];  // rank << P2MAXLOG | sub-bucket, or -1
 #pragma unroll
     for (int q = 0; q < RI; ++q) {
