@@ -40,7 +40,6 @@
 // sub-partitions.
 #include <algorithm>
 #include <climits>
-#include <cstddef>
 #include <string>
 #include <vector>
 
@@ -801,6 +800,11 @@ constexpr int P2TILE = P2T * P2I;  // rows a pass-2 tile
 #define PF_P2_RI2 6
 #endif
 constexpr int P2RI2 = PF_P2_RI2;
+// 1: the shared-memory path's first pass through the tile scatter when
+// B <= P2BINS (PF_FIRST_TILE=0|1 chooses at run time)
+#ifndef PF_FIRST_TILE
+#define PF_FIRST_TILE 1
+#endif
 constexpr int P2MAXLOG = 10;       // sub-buckets a partition splits into, log2, at most
 constexpr int P2BINS = 1 << P2MAXLOG;
 constexpr int P2BPT = P2BINS / P2T;  // sub-buckets a thread scans
@@ -1366,319 +1370,6 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
   if (bad_group) atomicAdd(&a.stats[2], bad_group);
 }
 
-// ---- the staged join: k_sjoin with its rows brought in by bulk copies ----
-//
-// One block of SJST threads a SM.  Thread 0 is the producer: it takes
-// sub-partitions from the counter one ahead of the block, and issues bulk
-// copies (one mbarrier a buffer, bounded waits) of the next sub-partition's
-// build rows into the build buffer as soon as the current build is done, and
-// of probe pieces (SJ_PIECE rows) into two piece buffers as soon as one is
-// consumed, so the loads of the next rows travel while the block builds,
-// probes and flushes.  A copy starts on a 16-byte boundary: the range is
-// widened to whole 16-byte words (the arrays carry slack at their ends) and
-// the rows are read from their offset.  Build rows past the first SJ_CAP of a
-// sub-partition are joined chunk by chunk with direct loads, each chunk
-// against all of its probe rows.
-#ifndef PF_SJ_STAGED
-#define PF_SJ_STAGED 0
-#endif
-// 1: the shared-memory path's first pass through the tile scatter when
-// B <= P2BINS (PF_FIRST_TILE=0|1 chooses at run time)
-#ifndef PF_FIRST_TILE
-#define PF_FIRST_TILE 1
-#endif
-constexpr int SJST = 1024;
-constexpr int SJ_PIECE = 2048;
-constexpr int SJ_BSLACK = 8;  // build staging rows beyond SJ_CAP (widening to 4-row words)
-
-struct SJStage {
-  long long key[SJ_TS];
-  SJSum sum[SJ_TS];
-  unsigned goff[SJ_TS];
-  unsigned cnt[SJ_TS];
-  long long pk[2][SJ_PIECE + 2];
-  long long pv[2][SJ_PIECE + 2];
-  long long bk[SJ_CAP + SJ_BSLACK];
-  int bg[SJ_CAP + SJ_BSLACK];
-  unsigned short slot_of[SJ_CAP];
-  uint64_t bar[3];  // piece buffers 0 and 1, the build buffer
-  long long cur[5], nxt[5];  // sub-partition, build rows [b0, b1), probe rows [p0, p1)
-  long long min_sum;
-  unsigned min_cnt, min_goff;
-  int has_min;
-};
-static_assert(offsetof(SJStage, pk) % 16 == 0 && offsetof(SJStage, pv) % 16 == 0 &&
-                  offsetof(SJStage, bk) % 16 == 0 && offsetof(SJStage, bg) % 16 == 0 &&
-                  ((SJ_PIECE + 2) * 8) % 16 == 0 && offsetof(SJStage, bar) % 8 == 0,
-              "bulk copy destinations on 16-byte boundaries");
-
-// The next sub-partition with rows on both sides, or d[0] = -1.
-__device__ void sj_fetch(const SJArgs& a, long long* d) {
-  while (true) {
-    const long long n = (long long)atomicAdd(a.counter, 1ULL);
-    if (n >= a.S) {
-      d[0] = -1;
-      return;
-    }
-    const long long b0 = (long long)a.bstart[n], b1 = (long long)a.bstart[n + 1];
-    const long long p0 = (long long)a.pstart[n], p1 = (long long)a.pstart[n + 1];
-    if (b1 > b0 && p1 > p0) {
-      d[0] = n;
-      d[1] = b0;
-      d[2] = b1;
-      d[3] = p0;
-      d[4] = p1;
-      return;
-    }
-  }
-}
-
-__device__ __forceinline__ long long sj_pieces(const long long* d) {
-  return (d[4] - d[3] + SJ_PIECE - 1) / SJ_PIECE;
-}
-
-__device__ void sj_issue_build(SJStage& S, const SJArgs& a, const long long* d) {
-  const long long r0 = d[1], r1 = min(d[2], d[1] + SJ_CAP);
-  const long long lo = r0 & ~3LL, hi = (r1 + 3) & ~3LL;
-  const unsigned bk = (unsigned)((hi - lo) * 8), bg = (unsigned)((hi - lo) * 4);
-  mbar_arrive_expect_tx(&S.bar[2], bk + bg);
-  bulk_g2s(S.bk, a.bkey + lo, bk, &S.bar[2]);
-  bulk_g2s(S.bg, a.bgrp + lo, bg, &S.bar[2]);
-}
-
-__device__ void sj_issue_piece(SJStage& S, const SJArgs& a, const long long* d, long long k,
-                               int buf) {
-  const long long r0 = d[3] + k * SJ_PIECE, r1 = min(d[4], r0 + SJ_PIECE);
-  const long long lo = r0 & ~1LL, hi = (r1 + 1) & ~1LL;
-  const unsigned bytes = (unsigned)((hi - lo) * 8);
-  mbar_arrive_expect_tx(&S.bar[buf], 2 * bytes);
-  bulk_g2s(S.pk[buf], a.pfk + lo, bytes, &S.bar[buf]);
-  bulk_g2s(S.pv[buf], a.pval + lo, bytes, &S.bar[buf]);
-}
-
-// Producer state, thread 0's registers.
-struct SJProducer {
-  int unit;            // 0: issuing the current sub-partition's pieces, 1: the next one's
-  long long piece;     // the next piece of that unit
-  long long issued;    // pieces issued so far (piece i goes to buffer i & 1)
-  long long builds;    // build copies issued so far
-  // Issue pieces while a buffer is free (consumed: pieces taken so far).
-  __device__ void pump(SJStage& S, const SJArgs& a, long long consumed) {
-    while (issued < consumed + 2) {
-      const long long* d = unit == 0 ? S.cur : S.nxt;
-      if (d[0] < 0) return;
-      if (piece < sj_pieces(d)) {
-        sj_issue_piece(S, a, d, piece, (int)(issued & 1));
-        ++piece;
-        ++issued;
-      } else if (unit == 0) {
-        unit = 1;
-        piece = 0;
-      } else {
-        return;
-      }
-    }
-  }
-};
-
-__device__ __forceinline__ void sj_insert(SJStage& S, long long key, int grp, int j,
-                                          const SJArgs& a, unsigned long long& bad_group) {
-  const long long g = (long long)grp - a.group_min;
-  unsigned goff = SJ_NONE;
-  if (g >= 0 && g < a.n_groups) goff = (unsigned)g;
-  else ++bad_group;
-  if (key == SJ_EMPTY) {
-    S.has_min = 1;
-    S.min_goff = goff;
-    S.slot_of[j] = 0xffff;
-    return;
-  }
-  unsigned t = sj_slot((uint64_t)key, a.logS);
-  for (int probes = 0; probes < SJ_TS; ++probes) {
-    const long long old = (long long)atomicCAS((unsigned long long*)&S.key[t],
-                                               (unsigned long long)SJ_EMPTY,
-                                               (unsigned long long)key);
-    if (old == SJ_EMPTY) {
-      S.goff[t] = goff;
-      break;
-    }
-    t = sj_next(t);
-  }
-  S.slot_of[j] = (unsigned short)t;
-}
-
-__device__ __forceinline__ void sj_lookup(SJStage& S, long long key, long long val, int logS,
-                                          unsigned long long& matched) {
-  if (key == SJ_EMPTY) {
-    if (S.has_min) {
-      atomicAdd((unsigned long long*)&S.min_sum, (unsigned long long)val);
-      atomicAdd(&S.min_cnt, 1u);
-      ++matched;
-    }
-    return;
-  }
-  unsigned t = sj_slot((uint64_t)key, logS);
-  for (int probes = 0; probes < SJ_TS; ++probes) {
-    const long long x = S.key[t];
-    if (x == SJ_EMPTY) return;
-    if (x == key) {
-      sj_sum_add(S.sum[t], val);
-      atomicAdd(&S.cnt[t], 1u);
-      ++matched;
-      return;
-    }
-    t = sj_next(t);
-  }
-}
-
-// Every build row of the chunk that matched into the slab; the table emptied.
-// Ends with the block synchronised.
-__device__ __forceinline__ void sj_flush(SJStage& S, const SJArgs& a, int nb) {
-  const int tid = threadIdx.x;
-  for (int j = tid; j < nb; j += SJST) {
-    const unsigned t = S.slot_of[j];
-    if (t == 0xffff) continue;
-    const unsigned c = S.cnt[t];
-    const unsigned go = S.goff[t];
-    if (c && go != SJ_NONE) {
-      atomicAdd(&a.slab[2 * (unsigned long long)go], sj_sum_get(S.sum[t]));
-      atomicAdd(&a.slab[2 * (unsigned long long)go + 1], (unsigned long long)c);
-    }
-    S.key[t] = SJ_EMPTY;
-    sj_sum_clear(S.sum[t]);
-    S.cnt[t] = 0;
-  }
-  if (tid == 0) {
-    if (S.has_min && S.min_cnt && S.min_goff != SJ_NONE) {
-      atomicAdd(&a.slab[2 * (unsigned long long)S.min_goff], (unsigned long long)S.min_sum);
-      atomicAdd(&a.slab[2 * (unsigned long long)S.min_goff + 1], (unsigned long long)S.min_cnt);
-    }
-    S.has_min = 0;
-    S.min_sum = 0;
-    S.min_cnt = 0;
-  }
-  __syncthreads();
-}
-
-__global__ void __launch_bounds__(SJST, 1) k_sjoin_staged(SJArgs a) {
-  extern __shared__ __align__(128) unsigned char sjs_smem[];
-  SJStage& S = *reinterpret_cast<SJStage*>(sjs_smem);
-  const int tid = threadIdx.x;
-  for (int t = tid; t < SJ_TS; t += SJST) {
-    S.key[t] = SJ_EMPTY;
-    sj_sum_clear(S.sum[t]);
-    S.cnt[t] = 0;
-  }
-  SJProducer pr{0, 0, 0, 0};
-  if (tid == 0) {
-    S.has_min = 0;
-    S.min_sum = 0;
-    S.min_cnt = 0;
-    for (int b = 0; b < 3; ++b) mbar_init(&S.bar[b], 1);
-    mbar_init_fence();
-    sj_fetch(a, S.cur);
-    if (S.cur[0] >= 0) {
-      sj_issue_build(S, a, S.cur);
-      pr.builds = 1;
-    }
-    sj_fetch(a, S.nxt);
-    pr.pump(S, a, 0);
-  }
-  __syncthreads();
-  unsigned long long matched = 0, bad_group = 0;
-  long long used = 0;   // pieces consumed
-  long long bused = 0;  // build buffers consumed
-  bool failed = false;
-  while (true) {
-    const long long s = S.cur[0];
-    const long long b0 = S.cur[1], b1 = S.cur[2], p0 = S.cur[3], p1 = S.cur[4];
-    if (s < 0) break;
-    // build the first chunk from the build buffer
-    const bool okb = mbar_wait_bounded(&S.bar[2], (unsigned)(bused & 1));
-    if (__syncthreads_or(!okb)) {
-      failed = true;
-      break;
-    }
-    ++bused;
-    const int nb0 = (int)min((long long)SJ_CAP, b1 - b0);
-    {
-      const int off = (int)(b0 & 3);
-      for (int j = tid; j < nb0; j += SJST)
-        sj_insert(S, S.bk[off + j], S.bg[off + j], j, a, bad_group);
-    }
-    __syncthreads();
-    if (tid == 0 && S.nxt[0] >= 0) {
-      fence_proxy_async_smem();
-      sj_issue_build(S, a, S.nxt);
-      ++pr.builds;
-    }
-    // probe the first chunk, piece by piece from the piece buffers
-    const long long np = sj_pieces(S.cur);
-    for (long long k = 0; k < np; ++k) {
-      const int buf = (int)(used & 1);
-      const bool okp = mbar_wait_bounded(&S.bar[buf], (unsigned)((used >> 1) & 1));
-      if (__syncthreads_or(!okp)) {
-        failed = true;
-        break;
-      }
-      const long long r0 = p0 + k * SJ_PIECE;
-      const int rows = (int)min((long long)SJ_PIECE, p1 - r0);
-      const int off = (int)(r0 & 1);
-      for (int i = tid; i < rows; i += SJST)
-        sj_lookup(S, S.pk[buf][off + i], S.pv[buf][off + i], a.logS, matched);
-      __syncthreads();
-      ++used;
-      if (tid == 0) {
-        fence_proxy_async_smem();
-        pr.pump(S, a, used);
-      }
-    }
-    if (failed) break;
-    // build rows past the first SJ_CAP: chunk by chunk, direct loads
-    int nb = nb0;
-    for (long long c0 = b0 + SJ_CAP; c0 < b1; c0 += SJ_CAP) {
-      sj_flush(S, a, nb);
-      nb = (int)min((long long)SJ_CAP, b1 - c0);
-      for (int j = tid; j < nb; j += SJST)
-        sj_insert(S, stream_ld(a.bkey + c0 + j), stream_ld(a.bgrp + c0 + j), j, a, bad_group);
-      __syncthreads();
-      for (long long i = p0 + tid; i < p1; i += SJST)
-        sj_lookup(S, stream_ld(a.pfk + i), stream_ld(a.pval + i), a.logS, matched);
-      __syncthreads();
-    }
-    sj_flush(S, a, nb);
-    // the next sub-partition becomes the current one
-    if (tid == 0) {
-      for (int q = 0; q < 5; ++q) S.cur[q] = S.nxt[q];
-      if (pr.unit == 1) {
-        pr.unit = 0;
-      } else {
-        pr.unit = 0;
-        pr.piece = 0;
-      }
-      if (S.cur[0] >= 0) sj_fetch(a, S.nxt);
-      else S.nxt[0] = -1;
-      fence_proxy_async_smem();
-      pr.pump(S, a, used);
-    }
-    __syncthreads();
-  }
-  if (failed) {
-    // a copy never landed: report it, let the copies in flight land, stop
-    if (tid == 0) {
-      atomicOr(&a.stats[1], 1ULL);
-      for (long long u = used; u < pr.issued; ++u)
-        mbar_wait_bounded(&S.bar[u & 1], (unsigned)((u >> 1) & 1), 1u << 16);
-      for (long long u = bused; u < pr.builds; ++u)
-        mbar_wait_bounded(&S.bar[2], (unsigned)(u & 1), 1u << 16);
-    }
-    __syncthreads();
-  }
-  for (int o = 16; o; o >>= 1) matched += __shfl_xor_sync(FULL, matched, o);
-  if ((tid & 31) == 0 && matched) atomicAdd(&a.stats[0], matched);
-  if (bad_group) atomicAdd(&a.stats[2], bad_group);
-}
-
 // PF_JOIN_PATH=rounds|smem picks the join path; read on every call (the
 // workspace size depends on it, so query and call must see the same value).
 int join_path_smem() {
@@ -1854,12 +1545,10 @@ JaLayout ja_layout(Arena& a, long long nb, long long np, int B, long long n_grou
     // finer than SJ_TARGET build rows
     l.s_max = (long long)B * std::min<long long>(
                                  P2BINS, (long long)pow2_at_least((uint64_t)(nb / SJ_TARGET + 1)));
-    // slack past the ends: the staged join's bulk copies widen their ranges
-    // to whole 16-byte words
-    l.pkey2 = a.take<long long>((size_t)nb + SJ_BSLACK);
-    l.pgrp2 = a.take<int>((size_t)nb + SJ_BSLACK);
-    l.pfk2 = a.take<long long>((size_t)np + 2);
-    l.pval2 = a.take<long long>((size_t)np + 2);
+    l.pkey2 = a.take<long long>(std::max<long long>(nb, 1));
+    l.pgrp2 = a.take<int>(std::max<long long>(nb, 1));
+    l.pfk2 = a.take<long long>(std::max<long long>(np, 1));
+    l.pval2 = a.take<long long>(std::max<long long>(np, 1));
     const long long rows[2] = {nb, np};
     for (int side = 0; side < 2; ++side) {
       l.nseg_max[side] = rows[side] / P2SEG + B + 1;
@@ -2080,13 +1769,7 @@ int join_smem(const JaLayout& l, int B, int logB, const long long* hc, long long
   a.stats = (unsigned long long*)stats_out;
   a.counter = l.sj_counter;
   PF_CUDA(cudaMemsetAsync(l.sj_counter, 0, sizeof(unsigned long long), st));
-  const char* se = getenv("PF_SJ_STAGED");
-  if (se ? se[0] != '0' : PF_SJ_STAGED) {
-    const size_t smem = sizeof(SJStage);
-    if (int rc = opt_in_smem((const void*)k_sjoin_staged, smem)) return rc;
-    PF_KERNEL("k_sjoin", st);
-    k_sjoin_staged<<<sms, SJST, smem, st>>>(a);
-  } else {
+  {
     const size_t smem = sizeof(SJSmem);
     if (int rc = opt_in_smem((const void*)k_sjoin, smem)) return rc;
     int per_sm = 0;
