@@ -162,16 +162,22 @@ __device__ __forceinline__ void adaptive_add(unsigned long long* slab, long long
 constexpr int CACHE_SLOTS = 1 << PF_CACHE_LOG;
 constexpr long long CACHE_EMPTY = -1;
 
+// A slot's sum is two 32-bit words (the low word's add returns its old value,
+// which shows the carry into the high word) and its count one: 64-bit adds on
+// shared memory cost far more than 32-bit ones, and a slot's count between
+// two flushes (one work item's rows) stays below 2^32.
 struct GroupCache {
   long long tag[CACHE_SLOTS];
-  unsigned long long sum[CACHE_SLOTS];
-  unsigned long long cnt[CACHE_SLOTS];
+  unsigned lo[CACHE_SLOTS];
+  unsigned hi[CACHE_SLOTS];
+  unsigned cnt[CACHE_SLOTS];
 };
 
 __device__ __forceinline__ void cache_init(GroupCache& gc) {
   for (int i = threadIdx.x; i < CACHE_SLOTS; i += blockDim.x) {
     gc.tag[i] = CACHE_EMPTY;
-    gc.sum[i] = 0;
+    gc.lo[i] = 0;
+    gc.hi[i] = 0;
     gc.cnt[i] = 0;
   }
 }
@@ -187,8 +193,11 @@ __device__ __forceinline__ void cache_add(GroupCache& gc, unsigned long long* sl
     t = old == CACHE_EMPTY ? g : old;
   }
   if (t == g) {
-    atomicAdd(&gc.sum[slot], sum);
-    atomicAdd(&gc.cnt[slot], cnt);
+    const unsigned l = (unsigned)sum, h = (unsigned)(sum >> 32);
+    const unsigned old = atomicAdd(&gc.lo[slot], l);
+    const unsigned hc = h + (old + l < old ? 1u : 0u);
+    if (hc) atomicAdd(&gc.hi[slot], hc);
+    atomicAdd(&gc.cnt[slot], (unsigned)cnt);
   } else {
     atomicAdd(&slab[2 * (unsigned long long)g], sum);
     atomicAdd(&slab[2 * (unsigned long long)g + 1], cnt);
@@ -200,10 +209,12 @@ __device__ __forceinline__ void cache_flush(GroupCache& gc, unsigned long long* 
   for (int i = threadIdx.x; i < CACHE_SLOTS; i += blockDim.x) {
     const long long g = gc.tag[i];
     if (g != CACHE_EMPTY) {
-      atomicAdd(&slab[2 * (unsigned long long)g], gc.sum[i]);
-      atomicAdd(&slab[2 * (unsigned long long)g + 1], gc.cnt[i]);
+      atomicAdd(&slab[2 * (unsigned long long)g],
+                ((unsigned long long)gc.hi[i] << 32) | gc.lo[i]);
+      atomicAdd(&slab[2 * (unsigned long long)g + 1], (unsigned long long)gc.cnt[i]);
       gc.tag[i] = CACHE_EMPTY;
-      gc.sum[i] = 0;
+      gc.lo[i] = 0;
+      gc.hi[i] = 0;
       gc.cnt[i] = 0;
     }
   }
