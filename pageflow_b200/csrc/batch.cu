@@ -189,7 +189,9 @@ __global__ void __launch_bounds__(BT2) k_batch(Header* h, const Desc* d, const i
     unsigned long long next = 0;
     if (PF_PREFETCH_ITEMS && threadIdx.x == 0) next = atomicAdd(&h->counter, 1ULL);
     const int inst = imap[it];
-    const Desc& D = d[inst];
+    // the instance's descriptor in registers for the item (read through a
+    // reference, every store to the tables or slabs would reload it)
+    const Desc D = d[inst];
     const long long local = it - D.item0;
     if (local < D.nbi) {
       // BV rows a thread at a time: loads, then every first claim, then the
