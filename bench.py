@@ -24,6 +24,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -915,6 +916,76 @@ def serve_cpu_baseline(spec, dims, fact, trace, seconds: float = 10.0):
                       f"{rows} probe rows, {t_run:.1f} s"}
 
 
+def drop_in_vs_reference(dev, timed, peak):
+    """The drop-in kernels against the reference's own CUDA kernels (its
+    operators/kernels/*.cu built from source for sm_100a), on the same
+    inputs, outputs checked equal: partition_sort of 50M rows (int64 key,
+    int64 and int32 payloads) into 256 padded buckets, and join_unique_hash
+    of 100M probe rows against 25M unique build keys (90% matching)."""
+    import torch
+    from oracle import plain_form
+    from pageflow_b200 import tqpkernels
+    if not plain_form.available():
+        return {"drop_in_vs_reference": "unavailable: the reference's kernels are not built"}
+    ref = plain_form.kernels()
+    g = torch.Generator(device=dev).manual_seed(11)
+    out = {}
+    n, B = 50_000_000, 256
+    cols = [torch.randint(-(1 << 40), 1 << 40, (n,), device=dev, generator=g),
+            torch.randint(-(1 << 40), 1 << 40, (n,), device=dev, generator=g),
+            torch.randint(-(1 << 30), 1 << 30, (n,), device=dev, generator=g, dtype=torch.int32)]
+    h1 = torch.zeros(B + 5, dtype=torch.int64, pin_memory=True)
+    h2 = torch.zeros(B + 5, dtype=torch.int64, pin_memory=True)
+    comp = [0, 0, 0]
+    a = tqpkernels.partition_sort(cols, comp, 0, None, n, 0, B, False, h1)
+    b = ref.partition_sort(cols, comp, 0, None, n, 0, B, False, h2)
+    torch.cuda.synchronize()
+    counts = h1[:B].tolist()
+
+    def real_rows(t):
+        # each bucket starts on a whole 512-byte unit of the column; padding
+        # rows are never written
+        rb = t.element_size() * (t.shape[1] if t.dim() == 2 else 1)
+        unit = 512 // math.gcd(rb, 512)
+        m = torch.zeros(t.shape[0], dtype=torch.bool, device=t.device)
+        at = 0
+        for c in counts:
+            m[at:at + c] = True
+            at += -(-c // unit) * unit
+        return m
+    same = h1[:B + 4].tolist() == h2[:B + 4].tolist() and len(a) == len(b) and all(
+        torch.equal(x[real_rows(x)], y[real_rows(y)]) for x, y in zip(a, b))
+    del a, b
+    ms = timed(lambda: tqpkernels.partition_sort(cols, comp, 0, None, n, 0, B, False, h1))
+    ms_ref = timed(lambda: ref.partition_sort(cols, comp, 0, None, n, 0, B, False, h2))
+    byts = n * (20 + 20 + 8)  # key read twice (count, scatter), columns read and written, gidx
+    out["partition_sort_50M_B256"] = {"ms": ms, "gbs": byts / ms / 1e6,
+                                      "frac": byts / ms / 1e6 / peak, "reference_ms": ms_ref,
+                                      "speedup": ms_ref / ms, "identical": same}
+    del cols
+    nb, np_ = 25_000_000, 100_000_000
+    bk = torch.randperm(nb, device=dev, generator=g).to(torch.int64) * 3 + 1
+    pick = torch.randint(0, nb, (np_,), device=dev, generator=g)
+    pk = bk[pick]
+    miss = torch.rand(np_, device=dev, generator=g) < 0.1
+    pk = torch.where(miss, pk + 1, pk)
+    h1, h2 = torch.zeros(2, dtype=torch.int64, pin_memory=True), torch.zeros(
+        2, dtype=torch.int64, pin_memory=True)
+    a = tqpkernels.join_unique_hash([bk], [pk], h1)
+    b = ref.join_unique_hash([bk], [pk], h2)
+    torch.cuda.synchronize()
+    m = int(h1[0])
+    same = m == int(h2[0]) and all(torch.equal(x[:m], y[:m]) for x, y in zip(a, b))
+    del a, b
+    ms = timed(lambda: tqpkernels.join_unique_hash([bk], [pk], h1))
+    ms_ref = timed(lambda: ref.join_unique_hash([bk], [pk], h2))
+    byts = nb * 8 + np_ * 8 + m * 16
+    out["join_unique_hash_25M_x_100M"] = {"ms": ms, "gbs": byts / ms / 1e6,
+                                          "frac": byts / ms / 1e6 / peak, "reference_ms": ms_ref,
+                                          "speedup": ms_ref / ms, "identical": same}
+    return out
+
+
 def run_kernels(args, world, rank, local_rank):
     """The operator primitives beside the fused path, each timed with CUDA
     events (median of `steps` runs after `warmup`) on inputs far above L2,
@@ -1024,6 +1095,8 @@ def run_kernels(args, world, rank, local_rank):
     out["group_hash_int64_int32"] = {"ms": ms, "gbs": byts / ms / 1e6,
                                      "frac": byts / ms / 1e6 / peak, "torch_ms": ms_ref,
                                      "identical": same}
+    del h, k1, k2, keys2
+    out.update(drop_in_vs_reference(dev, timed, peak))
     if rank == 0:
         line = {"metric": "operator primitives: ms per call (median) and GB/s of algorithmic bytes",
                 "value": out["gather_2x_int64"]["gbs"], "unit": "GB/s", "n_gpus": world,

@@ -4,14 +4,16 @@
 // operators/partition_sort.py:68-143).
 //
 // Work split.  The domain (the pre-mask rows, or the kept rows after the
-// select-first prologue) is cut into one contiguous CHUNK per CTA, a whole
-// number of 4096-row sub-tiles, about four CTAs per SM.  A CTA walks its
-// chunk sub-tile by sub-tile in row order, which keeps the partition stable
-// while each CTA owns a single run of every bucket:
+// select-first prologue) is cut into CHUNKS of one 2048-row sub-tile (more
+// only when the chunk histograms would pass 2^24 entries).  Every chunk owns
+// a single run of every bucket, at an offset the chunk histograms fix, which
+// keeps the partition stable; the scatter runs one CTA a chunk, so the chunks
+// at work at one time are neighbours:
 //
 //   k_hist      one histogram row per chunk, hist[chunk][b] (coalesced)
-//   k_scan      per bucket, exclusive offsets over the chunks (a warp per 32
-//               buckets, sixteen warps splitting the chunks)
+//   k_scan      per bucket, exclusive offsets over the chunks (k_scan_sum,
+//               k_scan_groups, k_scan_write: the chunks in 64 groups, each
+//               group's sums, a scan over the groups, the offsets)
 //   k_bases     bucket counts, each row-width class's padded bucket starts and
 //               total, all written into the caller's pinned host_out through
 //               its device alias; an overflow check against n_valid
@@ -41,15 +43,22 @@ namespace pf {
 namespace {
 
 constexpr int PT = 512;          // threads per CTA
-constexpr int PITEMS = 8;        // rows per thread per sub-tile
+#ifndef PF_PART_ITEMS
+#define PF_PART_ITEMS 4
+#endif
+#ifndef PF_PART_STAGE_RB
+#define PF_PART_STAGE_RB 8
+#endif
+// 2048-row sub-tiles staging at most 8 bytes a row keep the scatter's shared
+// memory small enough for several CTAs a SM
+constexpr int PITEMS = PF_PART_ITEMS;  // rows per thread per sub-tile
 constexpr int SUB = PT * PITEMS; // rows per sub-tile
 constexpr int PW = PT / 32;      // warps
 constexpr int WSEG = 32 * PITEMS;  // rows of a warp's segment of a sub-tile
 constexpr int MAXC = PF_PART_MAX_COLS;
 constexpr int MAXCLS = PF_PART_MAX_WIDTHS;
 constexpr int BMAX = PF_PART_B_MAX;
-constexpr int STAGE_MAX_RB = 32;  // rows up to this width are staged in smem
-constexpr int CHUNKS_PER_SM = 4;
+constexpr int STAGE_MAX_RB = PF_PART_STAGE_RB;  // rows up to this width are staged in smem
 
 struct Cols {
   const unsigned char* in[MAXC];
@@ -281,30 +290,77 @@ __global__ void __launch_bounds__(PT) k_hist(Params p) {
 
 // ---- K2: per-bucket offsets over the chunks ---------------------------------
 
-// Block g owns buckets [32g, 32g+32), lane = bucket; warp j scans chunks
-// [j*per, (j+1)*per).  counts[b] = the bucket's rows.
-__global__ void __launch_bounds__(PT) k_scan(int* __restrict__ hist, int nchunks, int B,
-                                             long long* __restrict__ counts, const int* flags) {
+// The chunks are cut into SCAN_G groups; block (x, y) owns buckets
+// [32x, 32x + 32) (lane = bucket) of group y, its warps splitting the group's
+// chunks.  k_scan_sum: each group's rows a bucket; k_scan_groups: per bucket,
+// each group's first row (exclusive over the groups) and counts[b], the
+// bucket's rows; k_scan_write: every chunk's exclusive offset into hist.
+constexpr int SCAN_G = 64;
+
+__device__ __forceinline__ void scan_range(int nchunks, int cg, int& c0, int& c1) {
+  const int g0 = blockIdx.y * cg, g1 = min(nchunks, g0 + cg);
+  const int per = (max(0, g1 - g0) + PW - 1) / PW;
+  c0 = min(g1, g0 + (threadIdx.x >> 5) * per);
+  c1 = min(g1, c0 + per);
+}
+
+__global__ void __launch_bounds__(PT) k_scan_sum(const int* __restrict__ hist, int nchunks, int B,
+                                                 int cg, long long* __restrict__ gsum,
+                                                 const int* flags) {
+  if (flags[0]) return;
+  __shared__ long long part[PW][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int b = blockIdx.x * 32 + lane;
+  int c0, c1;
+  scan_range(nchunks, cg, c0, c1);
+  long long s = 0;
+  if (b < B)
+    for (int c = c0; c < c1; ++c) s += hist[(long long)c * B + b];
+  part[w][lane] = s;
+  __syncthreads();
+  if (w == 0 && b < B) {
+    long long t = 0;
+    for (int j = 0; j < PW; ++j) t += part[j][lane];
+    gsum[(long long)blockIdx.y * B + b] = t;
+  }
+}
+
+__global__ void k_scan_groups(long long* __restrict__ gsum, int B, long long* __restrict__ counts,
+                              const int* flags) {
+  if (flags[0]) return;
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  long long run = 0;
+  for (int g = 0; g < SCAN_G; ++g) {
+    const long long t = gsum[(long long)g * B + b];
+    gsum[(long long)g * B + b] = run;
+    run += t;
+  }
+  counts[b] = run;
+}
+
+__global__ void __launch_bounds__(PT) k_scan_write(int* __restrict__ hist, int nchunks, int B,
+                                                   int cg, const long long* __restrict__ gsum,
+                                                   const int* flags) {
   if (flags[0]) return;
   __shared__ long long part[PW][32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int b = blockIdx.x * 32 + lane;
   const bool live = b < B;
-  const int per = (nchunks + PW - 1) / PW;
-  const int c0 = w * per, c1 = min(nchunks, c0 + per);
+  int c0, c1;
+  scan_range(nchunks, cg, c0, c1);
   long long s = 0;
   if (live)
     for (int c = c0; c < c1; ++c) s += hist[(long long)c * B + b];
   part[w][lane] = s;
   __syncthreads();
   if (w == 0) {
-    long long run = 0;
+    long long run = live ? gsum[(long long)blockIdx.y * B + b] : 0;
     for (int j = 0; j < PW; ++j) {
       const long long t = part[j][lane];
       part[j][lane] = run;
       run += t;
     }
-    if (live) counts[b] = run;
   }
   __syncthreads();
   if (live) {
@@ -400,6 +456,21 @@ __device__ __forceinline__ void stage_rows(const Params& p, int c, const bool (&
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const T* in = reinterpret_cast<const T*>(p.c.in[c]);
   const bool comp = p.c.comp[c] != 0;
+  if (nw == 1) {
+    // one word a row: every row's load issued before any is stored
+    T v[PITEMS];
+#pragma unroll
+    for (int k = 0; k < PITEMS; ++k) {
+      if (valid[k]) {
+        const long long i = sb + w * WSEG + k * 32 + lane;
+        v[k] = in[comp ? comp_index(p, i, kept_at + rank[k]) : raw_index(p, i)];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < PITEMS; ++k)
+      if (valid[k]) stage[slot[k]] = v[k];
+    return;
+  }
 #pragma unroll
   for (int k = 0; k < PITEMS; ++k) {
     if (valid[k]) {
@@ -419,7 +490,12 @@ __device__ __forceinline__ void write_runs(const Params& p, int c, const T* stag
   T* out = reinterpret_cast<T*>(p.c.out[c]);
   const int n = tvalid * nw;
   if (nw == 1) {
-    for (int e = threadIdx.x; e < n; e += PT) out[gbc[sbk[e]] + e] = stage[e];
+    // n <= SUB: PITEMS staged rows a thread, their lookups unrolled together
+#pragma unroll
+    for (int t = 0; t < PITEMS; ++t) {
+      const int e = t * PT + threadIdx.x;
+      if (e < n) out[gbc[sbk[e]] + e] = stage[e];
+    }
   } else {
     for (int e = threadIdx.x; e < n; e += PT) {
       const int s = e / nw, q = e - s * nw;
@@ -481,15 +557,17 @@ __global__ void __launch_bounds__(PT) k_scatter(Params p) {
   unsigned char* stage = smem + off;
 
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const int* hrow = p.hist + (long long)blockIdx.x * B;
-  for (int b = tid; b < B; b += PT) run[b] = hrow[b];
   for (int x = tid; x < PW * B; x += PT) wcnt[x] = 0;
+  const unsigned lt = lanemask_lt();
+  // the chunks in turn (chunk ch, ch + grid, ...)
+  for (int ch = blockIdx.x; ch < p.nchunks; ch += gridDim.x) {
+  const int* hrow = p.hist + (long long)ch * B;
+  for (int b = tid; b < B; b += PT) run[b] = hrow[b];
   __syncthreads();
 
-  const long long lo = (long long)blockIdx.x * p.chunk;
+  const long long lo = (long long)ch * p.chunk;
   const long long hi = min(p.ndom, lo + p.chunk);
-  long long kept_at = p.needs_j ? p.coff[blockIdx.x] : 0;
-  const unsigned lt = lanemask_lt();
+  long long kept_at = p.needs_j ? p.coff[ch] : 0;
 
   for (long long sb = lo; sb < hi; sb += SUB) {
     bool valid[PITEMS];
@@ -634,9 +712,10 @@ __global__ void __launch_bounds__(PT) k_scatter(Params p) {
     }
     {
       const long long* gbg = gb + p.gcls * B;
-      for (int s = tid; s < tvalid; s += PT) {
-        const long long i = sb + srow[s];
-        p.gout[gbg[sbk[s]] + s] = p.goff + raw_index(p, i);
+#pragma unroll
+      for (int t = 0; t < PITEMS; ++t) {
+        const int s = t * PT + tid;
+        if (s < tvalid) p.gout[gbg[sbk[s]] + s] = p.goff + raw_index(p, sb + srow[s]);
       }
     }
     __syncthreads();
@@ -645,13 +724,17 @@ __global__ void __launch_bounds__(PT) k_scatter(Params p) {
     kept_at += ktot;
     __syncthreads();
   }
+  }
 }
 
-// The chunking of an n-row domain: rows a CTA walks, and the CTAs.
-void chunking(long long n, long long* chunk, int* nchunks) {
+// The chunking of an n-row domain: one sub-tile a chunk, or as few sub-tiles
+// as keep the chunk histograms within 2^24 entries.  The scatter's CTAs walk
+// the chunks in turn, so the chunks at work at one time are neighbours and
+// write next to each other in every bucket (with a long chunk a CTA, every CTA
+// kept its own partly written lines in every bucket and column).
+void chunking(long long n, int B, long long* chunk, int* nchunks) {
   const long long subs = std::max<long long>(1, (n + SUB - 1) / SUB);
-  const long long want = std::max<long long>(1, (long long)sm_count() * CHUNKS_PER_SM);
-  const long long per = (subs + want - 1) / want;
+  const long long per = std::max<long long>(1, (subs * B + (1LL << 24) - 1) >> 24);
   *chunk = per * SUB;
   *nchunks = (int)std::max<long long>(1, (n + *chunk - 1) / *chunk);
 }
@@ -662,6 +745,7 @@ struct Layout {
   long long* ptotal;     // [1]
   int* src;              // [n_valid] select-first
   int* hist;             // [nchunks * B]
+  long long* gsum;       // [SCAN_G * B]
   long long* counts;     // [B]
   long long* bases;      // [MAXCLS * B]
 };
@@ -673,15 +757,16 @@ Layout layout(Arena& a, long long n_dom, long long n_valid, int B, bool has_mask
   l.ptotal = a.take<long long>(1);
   long long pchunk;
   int pn;
-  chunking(n_dom, &pchunk, &pn);
+  chunking(n_dom, B, &pchunk, &pn);
   l.pcnt = a.take<long long>(has_mask ? pn : 1);
   l.src = a.take<int>(has_mask && select_first ? std::max<long long>(1, n_valid) : 1);
   long long dom = has_mask && select_first ? n_valid : n_dom;
   long long chunk;
   int nch;
-  chunking(dom, &chunk, &nch);
+  chunking(dom, B, &chunk, &nch);
   if (pn > nch) nch = pn;
   l.hist = a.take<int>((size_t)nch * B);
+  l.gsum = a.take<long long>((size_t)SCAN_G * B);
   l.counts = a.take<long long>(B);
   l.bases = a.take<long long>((size_t)MAXCLS * B);
   return l;
@@ -787,7 +872,7 @@ extern "C" int pf_partition_sort(const void* const* cols_in, void* const* cols_o
   const bool prologue = use_sel || p.needs_j;
   long long pchunk;
   int pn;
-  chunking(n_dom, &pchunk, &pn);
+  chunking(n_dom, B, &pchunk, &pn);
   if (prologue && n_dom > 0) {
     {
       PF_KERNEL("k_mask_count", st);
@@ -820,7 +905,7 @@ extern "C" int pf_partition_sort(const void* const* cols_in, void* const* cols_o
     p.ndom = n_dom;
     p.coff = l.pcnt;
   }
-  chunking(p.ndom, &p.chunk, &p.nchunks);
+  chunking(p.ndom, B, &p.chunk, &p.nchunks);
   p.hist = l.hist;
   p.bases = l.bases;
 
@@ -830,8 +915,12 @@ extern "C" int pf_partition_sort(const void* const* cols_in, void* const* cols_o
   }
   PF_LAUNCH("k_hist");
   {
+    const int cg = (p.nchunks + SCAN_G - 1) / SCAN_G;
+    const dim3 grid((B + 31) / 32, SCAN_G);
     PF_KERNEL("k_scan", st);
-    k_scan<<<(B + 31) / 32, PT, 0, st>>>(l.hist, p.nchunks, B, l.counts, l.flags);
+    k_scan_sum<<<grid, PT, 0, st>>>(l.hist, p.nchunks, B, cg, l.gsum, l.flags);
+    k_scan_groups<<<(B + 255) / 256, 256, 0, st>>>(l.gsum, B, l.counts, l.flags);
+    k_scan_write<<<grid, PT, 0, st>>>(l.hist, p.nchunks, B, cg, l.gsum, l.flags);
   }
   PF_LAUNCH("k_scan");
   Rpu rpu;
@@ -849,6 +938,8 @@ extern "C" int pf_partition_sort(const void* const* cols_in, void* const* cols_o
   const size_t smem = scatter_smem(B, stage_rb);
   if (int rc = opt_in_smem((const void*)k_scatter, smem)) return rc;
   {
+    // one CTA a chunk: the block scheduler starts the next chunk's loads on a
+    // SM while the CTA there still writes out its own
     PF_KERNEL("k_scatter", st);
     k_scatter<<<p.nchunks, PT, smem, st>>>(p);
   }
