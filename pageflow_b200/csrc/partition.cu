@@ -288,6 +288,29 @@ __global__ void __launch_bounds__(PT) k_hist(Params p) {
   for (int b = tid; b < p.B; b += PT) row[b] = h[b];
 }
 
+// The histogram of the plain case (no mask, one sub-tile a chunk): every
+// thread's keys loaded first, then counted.
+__global__ void __launch_bounds__(PT) k_hist_plain(Params p) {
+  if (failed(p)) return;
+  __shared__ int h[BMAX];
+  const int tid = threadIdx.x;
+  for (int b = tid; b < p.B; b += PT) h[b] = 0;
+  const long long t0 = (long long)blockIdx.x * SUB;
+  long long kv[PITEMS];
+#pragma unroll
+  for (int k = 0; k < PITEMS; ++k) {
+    const long long i = t0 + k * PT + tid;
+    kv[k] = i < p.ndom ? p.key[i] : 0;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < PITEMS; ++k)
+    if (t0 + k * PT + tid < p.ndom) atomicAdd(&h[bucket_of_hash(mix64((uint64_t)kv[k]), p.logB)], 1);
+  __syncthreads();
+  int* row = p.hist + (long long)blockIdx.x * p.B;
+  for (int b = tid; b < p.B; b += PT) row[b] = h[b];
+}
+
 // ---- K2: per-bucket offsets over the chunks ---------------------------------
 
 // The chunks are cut into SCAN_G groups; block (x, y) owns buckets
@@ -536,6 +559,164 @@ size_t scatter_smem(int B, int stage_rb) {
   s = (s + 15) / 16 * 16;
   s += (size_t)SUB * stage_rb;   // stage
   return s;
+}
+
+// The scatter for the plain case: no mask, one sub-tile a chunk, every column
+// one word a row (1, 2, 4 or 8 bytes).  The same stable ranking and staging
+// as k_scatter with less state a thread: a CTA a chunk, its rows' buckets,
+// warp ranks, the tile's bucket runs, then each column loaded, staged and
+// written out with every thread's rows unrolled.
+struct PlainSmem {
+  unsigned long long stage[SUB];
+  long long gb[MAXCLS][BMAX];
+  int wh[PW][BMAX];
+  int tcnt[BMAX], tstart[BMAX];
+  unsigned short sbk[SUB], srow[SUB];
+  int wtot[PW];
+  int tvalid;
+};
+
+template <typename T>
+__device__ __forceinline__ void plain_column(PlainSmem& S, const unsigned char* in_,
+                                             unsigned char* out_, const long long* gbc,
+                                             long long t0, long long n, const int (&slot)[PITEMS],
+                                             const bool (&valid)[PITEMS], int tvalid) {
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const T* in = reinterpret_cast<const T*>(in_);
+  T* out = reinterpret_cast<T*>(out_);
+  T* stage = reinterpret_cast<T*>(S.stage);
+  T v[PITEMS];
+#pragma unroll
+  for (int k = 0; k < PITEMS; ++k)
+    if (valid[k]) v[k] = in[t0 + w * WSEG + k * 32 + lane];
+#pragma unroll
+  for (int k = 0; k < PITEMS; ++k)
+    if (valid[k]) stage[slot[k]] = v[k];
+  __syncthreads();
+#pragma unroll
+  for (int t = 0; t < PITEMS; ++t) {
+    const int e = t * PT + tid;
+    if (e < tvalid) out[gbc[S.sbk[e]] + e] = stage[e];
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(PT) k_scatter_plain(Params p) {
+  if (failed(p)) return;
+  extern __shared__ __align__(16) unsigned char plain_smem[];
+  PlainSmem& S = *reinterpret_cast<PlainSmem*>(plain_smem);
+  const int B = p.B;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const long long t0 = (long long)blockIdx.x * SUB;
+  for (int x = tid; x < PW * BMAX; x += PT) (&S.wh[0][0])[x] = 0;
+  bool valid[PITEMS];
+  int bk[PITEMS];
+  {
+    long long kv[PITEMS];
+#pragma unroll
+    for (int k = 0; k < PITEMS; ++k) {
+      const long long i = t0 + w * WSEG + k * 32 + lane;
+      valid[k] = i < p.ndom;
+      kv[k] = valid[k] ? p.key[i] : 0;
+    }
+#pragma unroll
+    for (int k = 0; k < PITEMS; ++k)
+      bk[k] = valid[k] ? bucket_of_hash(mix64((uint64_t)kv[k]), p.logB) : -1;
+  }
+  __syncthreads();
+  // stable rank inside (warp, bucket): lane order within an item, items in order
+  int sk[PITEMS];
+  {
+    const unsigned lt = lanemask_lt();
+#pragma unroll
+    for (int k = 0; k < PITEMS; ++k) {
+      const unsigned peers = __match_any_sync(FULL, bk[k]);
+      const int before = __popc(peers & lt);
+      const int base = bk[k] >= 0 ? S.wh[w][bk[k]] : 0;
+      __syncwarp();
+      if (bk[k] >= 0 && before == 0) S.wh[w][bk[k]] = base + __popc(peers);
+      __syncwarp();
+      sk[k] = base + before;
+    }
+  }
+  __syncthreads();
+  // each warp's start inside the tile's run of every bucket
+  for (int b = tid; b < B; b += PT) {
+    int r = 0;
+#pragma unroll
+    for (int q = 0; q < PW; ++q) {
+      const int t = S.wh[q][b];
+      S.wh[q][b] = r;
+      r += t;
+    }
+    S.tcnt[b] = r;
+  }
+  __syncthreads();
+  // the tile's bucket runs in bucket order (B <= PT: a bucket a thread)
+  {
+    const int v = tid < B ? S.tcnt[tid] : 0;
+    int incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) S.wtot[w] = incl;
+    __syncthreads();
+    int pre = 0, tot = 0;
+#pragma unroll
+    for (int q = 0; q < PW; ++q) {
+      const int t = S.wtot[q];
+      pre += q < w ? t : 0;
+      tot += t;
+    }
+    if (tid < B) S.tstart[tid] = pre + incl - v;
+    if (tid == 0) S.tvalid = tot;
+    __syncthreads();
+  }
+  const int* hrow = p.hist + (long long)blockIdx.x * B;
+  for (int x = tid; x < p.ncls * B; x += PT) {
+    const int cl = x / B, b = x - cl * B;
+    S.gb[cl][b] = p.bases[(long long)cl * B + b] + hrow[b] - S.tstart[b];
+  }
+  int slot[PITEMS];
+#pragma unroll
+  for (int k = 0; k < PITEMS; ++k) {
+    slot[k] = 0;
+    if (bk[k] >= 0) {
+      const int s = S.tstart[bk[k]] + S.wh[w][bk[k]] + sk[k];
+      slot[k] = s;
+      S.sbk[s] = (unsigned short)bk[k];
+      S.srow[s] = (unsigned short)(w * WSEG + k * 32 + lane);
+    }
+  }
+  __syncthreads();
+  const int tvalid = S.tvalid;
+  for (int c = 0; c < p.c.ncols; ++c) {
+    const long long* gbc = S.gb[p.c.cls[c]];
+    switch (p.c.rb[c]) {
+      case 8:
+        plain_column<unsigned long long>(S, p.c.in[c], p.c.out[c], gbc, t0, p.ndom, slot, valid,
+                                         tvalid);
+        break;
+      case 4:
+        plain_column<unsigned>(S, p.c.in[c], p.c.out[c], gbc, t0, p.ndom, slot, valid, tvalid);
+        break;
+      case 2:
+        plain_column<unsigned short>(S, p.c.in[c], p.c.out[c], gbc, t0, p.ndom, slot, valid,
+                                     tvalid);
+        break;
+      default:
+        plain_column<unsigned char>(S, p.c.in[c], p.c.out[c], gbc, t0, p.ndom, slot, valid,
+                                    tvalid);
+        break;
+    }
+  }
+  const long long* gbg = S.gb[p.gcls];
+#pragma unroll
+  for (int t = 0; t < PITEMS; ++t) {
+    const int e = t * PT + tid;
+    if (e < tvalid) p.gout[gbg[S.sbk[e]] + e] = p.goff + t0 + S.srow[e];
+  }
 }
 
 __global__ void __launch_bounds__(PT) k_scatter(Params p) {
@@ -909,9 +1090,16 @@ extern "C" int pf_partition_sort(const void* const* cols_in, void* const* cols_o
   p.hist = l.hist;
   p.bases = l.bases;
 
+  // the plain case: no mask, one sub-tile a chunk, one word a row
+  bool plain = !p.mask && !p.src && !p.needs_j && p.chunk == SUB && !p.key_comp &&
+               getenv("PF_PART_GENERAL") == nullptr;
+  for (int c = 0; c < p.c.ncols; ++c)
+    plain = plain && !p.c.comp[c] && p.c.word[c] == p.c.rb[c] &&
+            (p.c.rb[c] == 1 || p.c.rb[c] == 2 || p.c.rb[c] == 4 || p.c.rb[c] == 8);
   {
     PF_KERNEL("k_hist", st);
-    k_hist<<<p.nchunks, PT, 0, st>>>(p);
+    if (plain) k_hist_plain<<<p.nchunks, PT, 0, st>>>(p);
+    else k_hist<<<p.nchunks, PT, 0, st>>>(p);
   }
   PF_LAUNCH("k_hist");
   {
@@ -935,6 +1123,18 @@ extern "C" int pf_partition_sort(const void* const* cols_in, void* const* cols_o
   cudaEvent_t ev;
   if (int rc = record_event(st, &ev)) return rc;
 
+  if (plain) {
+    const size_t smem = sizeof(PlainSmem);
+    if (int rc = opt_in_smem((const void*)k_scatter_plain, smem)) return rc;
+    {
+      PF_KERNEL("k_scatter", st);
+      k_scatter_plain<<<p.nchunks, PT, smem, st>>>(p);
+    }
+    PF_LAUNCH("k_scatter");
+    // the call's one host wait: the counts, while the scatter runs
+    if (int rc = wait_event(ev)) return rc;
+    return ok();
+  }
   const size_t smem = scatter_smem(B, stage_rb);
   if (int rc = opt_in_smem((const void*)k_scatter, smem)) return rc;
   {
