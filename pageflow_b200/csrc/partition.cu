@@ -576,32 +576,65 @@ struct PlainSmem {
   int tvalid;
 };
 
-template <typename T>
-__device__ __forceinline__ void plain_column(PlainSmem& S, const unsigned char* in_,
-                                             unsigned char* out_, const long long* gbc,
-                                             long long t0, long long n, const int (&slot)[PITEMS],
-                                             const bool (&valid)[PITEMS], int tvalid) {
+// A column of the plain case moves in three steps: its rows loaded into
+// registers (widened to 8 bytes), staged in bucket order, written out. The
+// next column's loads are issued before this column's write-out.
+__device__ __forceinline__ void plain_load(const Params& p, int c, long long t0,
+                                           const bool (&valid)[PITEMS],
+                                           unsigned long long (&v)[PITEMS]) {
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const T* in = reinterpret_cast<const T*>(in_);
-  T* out = reinterpret_cast<T*>(out_);
-  T* stage = reinterpret_cast<T*>(S.stage);
-  T v[PITEMS];
+  const unsigned char* in = p.c.in[c];
+  const long long r0 = t0 + w * WSEG + lane;
+  switch (p.c.rb[c]) {
+    case 8:
 #pragma unroll
-  for (int k = 0; k < PITEMS; ++k)
-    if (valid[k]) v[k] = in[t0 + w * WSEG + k * 32 + lane];
+      for (int k = 0; k < PITEMS; ++k)
+        if (valid[k]) v[k] = reinterpret_cast<const unsigned long long*>(in)[r0 + k * 32];
+      break;
+    case 4:
 #pragma unroll
-  for (int k = 0; k < PITEMS; ++k)
-    if (valid[k]) stage[slot[k]] = v[k];
-  __syncthreads();
+      for (int k = 0; k < PITEMS; ++k)
+        if (valid[k]) v[k] = reinterpret_cast<const unsigned*>(in)[r0 + k * 32];
+      break;
+    case 2:
 #pragma unroll
-  for (int t = 0; t < PITEMS; ++t) {
-    const int e = t * PT + tid;
-    if (e < tvalid) out[gbc[S.sbk[e]] + e] = stage[e];
+      for (int k = 0; k < PITEMS; ++k)
+        if (valid[k]) v[k] = reinterpret_cast<const unsigned short*>(in)[r0 + k * 32];
+      break;
+    default:
+#pragma unroll
+      for (int k = 0; k < PITEMS; ++k)
+        if (valid[k]) v[k] = in[r0 + k * 32];
+      break;
   }
-  __syncthreads();
 }
 
-__global__ void __launch_bounds__(PT) k_scatter_plain(Params p) {
+template <typename T>
+__device__ __forceinline__ void plain_stage(PlainSmem& S, const int (&slot)[PITEMS],
+                                            const bool (&valid)[PITEMS],
+                                            const unsigned long long (&v)[PITEMS]) {
+  T* stage = reinterpret_cast<T*>(S.stage);
+#pragma unroll
+  for (int k = 0; k < PITEMS; ++k)
+    if (valid[k]) stage[slot[k]] = (T)v[k];
+}
+
+template <typename T>
+__device__ __forceinline__ void plain_write(const PlainSmem& S, unsigned char* out_,
+                                            const long long* gbc, int tvalid) {
+  const T* stage = reinterpret_cast<const T*>(S.stage);
+  T* out = reinterpret_cast<T*>(out_);
+#pragma unroll
+  for (int t = 0; t < PITEMS; ++t) {
+    const int e = t * PT + threadIdx.x;
+    if (e < tvalid) out[gbc[S.sbk[e]] + e] = stage[e];
+  }
+}
+
+#ifndef PF_PART_PLAIN_MINB
+#define PF_PART_PLAIN_MINB 1
+#endif
+__global__ void __launch_bounds__(PT, PF_PART_PLAIN_MINB) k_scatter_plain(Params p) {
   if (failed(p)) return;
   extern __shared__ __align__(16) unsigned char plain_smem[];
   PlainSmem& S = *reinterpret_cast<PlainSmem*>(plain_smem);
@@ -611,6 +644,7 @@ __global__ void __launch_bounds__(PT) k_scatter_plain(Params p) {
   for (int x = tid; x < PW * BMAX; x += PT) (&S.wh[0][0])[x] = 0;
   bool valid[PITEMS];
   int bk[PITEMS];
+  unsigned long long v[PITEMS];
   {
     long long kv[PITEMS];
 #pragma unroll
@@ -618,6 +652,13 @@ __global__ void __launch_bounds__(PT) k_scatter_plain(Params p) {
       const long long i = t0 + w * WSEG + k * 32 + lane;
       valid[k] = i < p.ndom;
       kv[k] = valid[k] ? p.key[i] : 0;
+    }
+    // the first column rides with the keys (the key column itself: no reload)
+    if ((const void*)p.c.in[0] == (const void*)p.key && p.c.rb[0] == 8) {
+#pragma unroll
+      for (int k = 0; k < PITEMS; ++k) v[k] = (unsigned long long)kv[k];
+    } else {
+      plain_load(p, 0, t0, valid, v);
     }
 #pragma unroll
     for (int k = 0; k < PITEMS; ++k)
@@ -693,23 +734,23 @@ __global__ void __launch_bounds__(PT) k_scatter_plain(Params p) {
   const int tvalid = S.tvalid;
   for (int c = 0; c < p.c.ncols; ++c) {
     const long long* gbc = S.gb[p.c.cls[c]];
-    switch (p.c.rb[c]) {
-      case 8:
-        plain_column<unsigned long long>(S, p.c.in[c], p.c.out[c], gbc, t0, p.ndom, slot, valid,
-                                         tvalid);
-        break;
-      case 4:
-        plain_column<unsigned>(S, p.c.in[c], p.c.out[c], gbc, t0, p.ndom, slot, valid, tvalid);
-        break;
-      case 2:
-        plain_column<unsigned short>(S, p.c.in[c], p.c.out[c], gbc, t0, p.ndom, slot, valid,
-                                     tvalid);
-        break;
-      default:
-        plain_column<unsigned char>(S, p.c.in[c], p.c.out[c], gbc, t0, p.ndom, slot, valid,
-                                    tvalid);
-        break;
+    const int rb = p.c.rb[c];
+    unsigned char* out = p.c.out[c];
+    switch (rb) {
+      case 8: plain_stage<unsigned long long>(S, slot, valid, v); break;
+      case 4: plain_stage<unsigned>(S, slot, valid, v); break;
+      case 2: plain_stage<unsigned short>(S, slot, valid, v); break;
+      default: plain_stage<unsigned char>(S, slot, valid, v); break;
     }
+    __syncthreads();
+    if (c + 1 < p.c.ncols) plain_load(p, c + 1, t0, valid, v);
+    switch (rb) {
+      case 8: plain_write<unsigned long long>(S, out, gbc, tvalid); break;
+      case 4: plain_write<unsigned>(S, out, gbc, tvalid); break;
+      case 2: plain_write<unsigned short>(S, out, gbc, tvalid); break;
+      default: plain_write<unsigned char>(S, out, gbc, tvalid); break;
+    }
+    __syncthreads();
   }
   const long long* gbg = S.gb[p.gcls];
 #pragma unroll
