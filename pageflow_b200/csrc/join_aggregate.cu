@@ -1446,16 +1446,14 @@ __global__ void __launch_bounds__(CT) k_gemit(const long long* __restrict__ sum,
   int rank[CITEMS];
 #pragma unroll
   for (int k = 0; k < CITEMS; ++k) kp[k] = base + k < n && count[base + k] > 0;
-  block_ranks(kp, rank, wsum);
-  const long long o = boff[blockIdx.x];
-#pragma unroll
-  for (int k = 0; k < CITEMS; ++k) {
-    if (kp[k]) {
-      const long long j = o + rank[k];
-      keys[j] = group_min + base + k;
-      sums[j] = sum[base + k];
-      counts[j] = count[base + k];
-    }
+  __shared__ unsigned short rows[CB];
+  const int tot = block_compact(kp, rank, rows, wsum);
+  const long long o = boff[blockIdx.x], b0 = (long long)blockIdx.x * CB;
+  for (int e = threadIdx.x; e < tot; e += CT) {
+    const long long r = b0 + rows[e];
+    keys[o + e] = group_min + r;
+    sums[o + e] = sum[r];
+    counts[o + e] = count[r];
   }
 }
 

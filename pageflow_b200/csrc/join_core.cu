@@ -130,14 +130,21 @@ __global__ void __launch_bounds__(CT) k_uh_emit(const int* __restrict__ partner,
   }
 #pragma unroll
   for (int k = 0; k < CITEMS; ++k) keep[k] = part[k] >= 0;
-  block_ranks(keep, rank, wsum);
-  const long long o = boff[blockIdx.x];
+  __shared__ unsigned short rows[CB];
+  __shared__ int sp[CB];
+  const int tot = block_ranks(keep, rank, wsum);
 #pragma unroll
   for (int k = 0; k < CITEMS; ++k) {
     if (keep[k]) {
-      build_idx[o + rank[k]] = part[k];
-      probe_idx[o + rank[k]] = base + k;
+      rows[rank[k]] = (unsigned short)(threadIdx.x * CITEMS + k);
+      sp[rank[k]] = part[k];
     }
+  }
+  __syncthreads();
+  const long long o = boff[blockIdx.x], b0 = (long long)blockIdx.x * CB;
+  for (int e = threadIdx.x; e < tot; e += CT) {
+    build_idx[o + e] = sp[e];
+    probe_idx[o + e] = b0 + rows[e];
   }
 }
 
@@ -247,11 +254,10 @@ __global__ void __launch_bounds__(CT) k_keep_emit(const unsigned char* __restric
 #pragma unroll
     for (int k = 0; k < CITEMS; ++k) kp[k] = base + k < n && keep[base + k];
   }
-  block_ranks(kp, rank, wsum);
-  const long long o = boff[blockIdx.x];
-#pragma unroll
-  for (int k = 0; k < CITEMS; ++k)
-    if (kp[k]) out[o + rank[k]] = base + k;
+  __shared__ unsigned short rows[CB];
+  const int tot = block_compact(kp, rank, rows, wsum);
+  const long long o = boff[blockIdx.x], b0 = (long long)blockIdx.x * CB;
+  for (int e = threadIdx.x; e < tot; e += CT) out[o + e] = b0 + rows[e];
 }
 
 __global__ void k_fill_i64(long long* p, long long v, long long n) {

@@ -10,6 +10,7 @@ namespace pf {
 constexpr int CT = 256;          // threads of a compaction block
 constexpr int CITEMS = 16;       // rows a thread
 constexpr int CB = CT * CITEMS;  // rows a compaction block covers
+static_assert(CB <= 65536, "block-local rows are 16-bit");
 
 // Exclusive scan in place of n int64 values by one block of 1024 threads;
 // the total goes to *total (device) and, when host is not null, to *host.
@@ -55,6 +56,20 @@ __device__ __forceinline__ int block_ranks(const bool (&keep)[CITEMS], int (&ran
     rank[k] = r;
     r += keep[k];
   }
+  __syncthreads();
+  return tot;
+}
+
+// block_ranks, then each kept row's block-local index (t*CITEMS + k) staged
+// at its rank in rows[] (shared memory, CB entries), so that the block writes
+// its kept rows out with consecutive threads on consecutive outputs.  Returns
+// the block's total; rows[] is complete on return.
+__device__ __forceinline__ int block_compact(const bool (&keep)[CITEMS], int (&rank)[CITEMS],
+                                             unsigned short* rows, int* wsum) {
+  const int tot = block_ranks(keep, rank, wsum);
+#pragma unroll
+  for (int k = 0; k < CITEMS; ++k)
+    if (keep[k]) rows[rank[k]] = (unsigned short)(threadIdx.x * CITEMS + k);
   __syncthreads();
   return tot;
 }

@@ -132,22 +132,22 @@ __global__ void __launch_bounds__(CT) k_occ_emit(FinishArgs a) {
   int rank[CITEMS];
 #pragma unroll
   for (int k = 0; k < CITEMS; ++k) kp[k] = base + k < a.cap && a.occ[base + k] != 0;
-  block_ranks(kp, rank, wsum);
-  const long long o = a.boff[blockIdx.x];
-  for (int k = 0; k < CITEMS; ++k) {
-    if (!kp[k]) continue;
-    const long long j = o + rank[k], slot = base + k;
+  __shared__ unsigned short rows[CB];
+  const int tot = block_compact(kp, rank, rows, wsum);
+  const long long o = a.boff[blockIdx.x], b0 = (long long)blockIdx.x * CB;
+  for (int e = threadIdx.x; e < tot; e += CT) {
+    const long long j = o + e, slot = b0 + rows[e];
     a.keys_out[j] = a.key_min + slot;
     for (int v = 0; v < a.nvals; ++v) {
       const int w = a.width[v];
       if (a.esize[v] == 8) {
         const long long* src = reinterpret_cast<const long long*>(a.values[v]);
         long long* dst = reinterpret_cast<long long*>(a.outs[v]);
-        for (int e = 0; e < w; ++e) dst[j * w + e] = src[slot * w + e];
+        for (int x = 0; x < w; ++x) dst[j * w + x] = src[slot * w + x];
       } else {
         const int* src = reinterpret_cast<const int*>(a.values[v]);
         int* dst = reinterpret_cast<int*>(a.outs[v]);
-        for (int e = 0; e < w; ++e) dst[j * w + e] = src[slot * w + e];
+        for (int x = 0; x < w; ++x) dst[j * w + x] = src[slot * w + x];
       }
     }
   }
