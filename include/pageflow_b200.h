@@ -126,9 +126,8 @@ int pf_join_unique_hash(const int64_t* build0, const int64_t* build1, int64_t n_
  * not allocate: no workspace argument and no device allocation by the
  * library; its scratch is one fixed device array of
  * PF_UH_STATIC_SCRATCH_BYTES (8 MiB + 64 KiB) inside the library, enough for
- * 262144 build rows with 1048576 probe rows (the table takes 16 bytes per
- * build row rounded up to a power of two, the partners 4 bytes per probe
- * row).  Larger calls return PF_EINVAL before anything is queued.  The match
+ * 524288 build rows with 1048576 probe rows (the table takes 8 bytes per
+ * build row, the partners 4 bytes per probe row).  Larger calls return PF_EINVAL before anything is queued.  The match
  * count goes to match_count (device int64[1]) on the stream; nothing waits.
  * The first call on a device, with that device current, sets the scratch up
  * (looks up its device address, loading the library's module there); make

@@ -3,8 +3,9 @@
 // wrapper operators/join_core.py):
 //
 //   unique hash  inner join on a build tuple (1-2 int64 keys) proven unique:
-//                a table of 8-byte slots (build row | 32-bit fingerprint of the
-//                tuple hash), at most half full, linear probing; each probe
+//                a table of 2*n_build 4-byte slots (the build row in the low
+//                r bits, r the bit width of n_build; the tuple hash's bits
+//                above them as a fingerprint), linear probing; each probe
 //                row's partner; the matched probe rows compacted in order
 //   semi / anti  a set of the build keys (INT64_MIN marks an empty slot), with
 //                an optional per-key min / max of one build column answering
@@ -26,7 +27,7 @@ namespace pf {
 namespace {
 
 constexpr int T = 256;
-constexpr unsigned long long EMPTY_SLOT = ~0ULL;
+constexpr unsigned EMPTY_SLOT = ~0u;
 constexpr long long EMPTY_KEY = LLONG_MIN;
 
 __device__ __forceinline__ uint64_t tuple_hash(long long k0, long long k1, bool two) {
@@ -41,67 +42,141 @@ __device__ __forceinline__ uint64_t first_slot(uint64_t h, int logcap) {
 }
 
 // ---- unique hash -------------------------------------------------------------
+//
+// A slot holds (hash << r) | row, rmask = 2^r - 1 with n_build <= rmask: a
+// row never fills its r bits, so no entry is all ones (EMPTY_SLOT).  The home
+// slot is the multiply-shift of the hash's bits below its top nine onto
+// [0, cap) (reference operators/kernels/join_core.cu:55 slot_of), which
+// leans on the high bits; the fingerprint takes the low ones.
+
+struct UhTable {
+  unsigned* slot;
+  unsigned long long cap;
+  unsigned rmask;
+  int rbits;
+};
+
+__device__ __forceinline__ unsigned long long uh_home(uint64_t h, unsigned long long cap) {
+  return __umul64hi(h << 9, cap);
+}
+
+__device__ __forceinline__ unsigned long long uh_next(unsigned long long s,
+                                                      unsigned long long cap) {
+  return s + 1 == cap ? 0 : s + 1;
+}
 
 template <bool TWO>
 __global__ void __launch_bounds__(T) k_uh_build(const long long* __restrict__ b0,
                                                 const long long* __restrict__ b1, long long n,
-                                                unsigned long long* table, int logcap) {
+                                                UhTable t) {
   const long long i = (long long)blockIdx.x * T + threadIdx.x;
   if (i >= n) return;
   const uint64_t h = tuple_hash(b0[i], TWO ? b1[i] : 0, TWO);
-  const uint64_t mask = (1ULL << logcap) - 1;
-  const unsigned long long entry = ((unsigned long long)(uint32_t)h << 32) | (uint32_t)i;
-  uint64_t s = first_slot(h, logcap);
-  for (uint64_t probes = 0; probes <= mask; ++probes) {
-    if (atomicCAS(&table[s], EMPTY_SLOT, entry) == EMPTY_SLOT) return;
-    s = (s + 1) & mask;
+  const unsigned entry = ((unsigned)h << t.rbits) | (unsigned)i;
+  unsigned long long s = uh_home(h, t.cap);
+  for (unsigned long long probes = 0; probes < t.cap; ++probes) {
+    if (atomicCAS(&t.slot[s], EMPTY_SLOT, entry) == EMPTY_SLOT) return;
+    s = uh_next(s, t.cap);
   }
 }
 
+#ifndef PF_UH_U
+#define PF_UH_U 2
+#endif
+constexpr int UH_U = PF_UH_U;  // probe rows a thread resolves together
+static_assert(CITEMS % UH_U == 0, "probe batches tile a thread's rows");
+
 // Probe CB rows a block: partner[i] (build row or -1), the block's matches.
+// UH_U rows at a time: their home and next slots loaded together, then their
+// candidates' keys; a row that those two slots do not settle walks on.
 template <bool TWO>
 __global__ void __launch_bounds__(CT) k_uh_probe(const long long* __restrict__ b0,
                                                  const long long* __restrict__ b1,
                                                  const long long* __restrict__ p0,
                                                  const long long* __restrict__ p1, long long n,
-                                                 const unsigned long long* __restrict__ table,
-                                                 int logcap, int* __restrict__ partner,
+                                                 UhTable t, int* __restrict__ partner,
                                                  long long* __restrict__ bcnt) {
-  const uint64_t mask = (1ULL << logcap) - 1;
+  const unsigned* __restrict__ tab = t.slot;
+  const unsigned fmask = ~t.rmask;
   const long long base = (long long)blockIdx.x * CB;
   int c = 0;
-#pragma unroll 4
-  for (int k = 0; k < CITEMS; ++k) {
-    const long long i = base + k * CT + threadIdx.x;
-    if (i >= n) break;
-    const long long k0 = p0[i], k1 = TWO ? p1[i] : 0;
-    const uint64_t h = tuple_hash(k0, k1, TWO);
-    const uint32_t fp = (uint32_t)h;
-    uint64_t s = first_slot(h, logcap);
-    int r = -1;
-    for (uint64_t probes = 0; probes <= mask; ++probes) {
-      const unsigned long long e = table[s];
-      if (e == EMPTY_SLOT) break;
-      if ((uint32_t)(e >> 32) == fp) {
-        const int row = (int)(uint32_t)e;
-        if (b0[row] == k0 && (!TWO || b1[row] == k1)) {
-          r = row;
-          break;
+  for (int kk = 0; kk < CITEMS; kk += UH_U) {
+    long long k0[UH_U], k1[UH_U];
+    unsigned fp[UH_U], e0[UH_U], e1[UH_U];
+    unsigned long long s0[UH_U];
+    int cand[UH_U], r[UH_U];
+#pragma unroll
+    for (int u = 0; u < UH_U; ++u) {
+      const long long i = base + (kk + u) * CT + threadIdx.x;
+      k0[u] = i < n ? p0[i] : 0;
+      k1[u] = TWO && i < n ? p1[i] : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < UH_U; ++u) {
+      const uint64_t h = tuple_hash(k0[u], k1[u], TWO);
+      fp[u] = (unsigned)h << t.rbits;
+      s0[u] = uh_home(h, t.cap);
+    }
+#pragma unroll
+    for (int u = 0; u < UH_U; ++u) {
+      const bool in = base + (kk + u) * CT + threadIdx.x < n;
+      e0[u] = in ? tab[s0[u]] : EMPTY_SLOT;
+      e1[u] = in ? tab[uh_next(s0[u], t.cap)] : EMPTY_SLOT;
+    }
+    // the candidate among the two slots: -1 settled as no match, -2 walk on
+#pragma unroll
+    for (int u = 0; u < UH_U; ++u) {
+      if (e0[u] == EMPTY_SLOT) cand[u] = -1;
+      else if ((e0[u] & fmask) == fp[u]) cand[u] = (int)(e0[u] & t.rmask);
+      else if (e1[u] == EMPTY_SLOT) cand[u] = -1;
+      else if ((e1[u] & fmask) == fp[u]) cand[u] = (int)(e1[u] & t.rmask);
+      else cand[u] = -2;
+    }
+    long long c0[UH_U], c1[UH_U];
+#pragma unroll
+    for (int u = 0; u < UH_U; ++u) {
+      c0[u] = cand[u] >= 0 ? b0[cand[u]] : 0;
+      c1[u] = TWO && cand[u] >= 0 ? b1[cand[u]] : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < UH_U; ++u) {
+      r[u] = -1;
+      if (cand[u] >= 0 && c0[u] == k0[u] && (!TWO || c1[u] == k1[u])) r[u] = cand[u];
+      else if (cand[u] != -1) {
+        // a fingerprint that matched another key, or two full slots: walk
+        // the chain from its home slot
+        unsigned long long s = s0[u];
+        for (unsigned long long probes = 0; probes < t.cap; ++probes) {
+          const unsigned e = tab[s];
+          if (e == EMPTY_SLOT) break;
+          if ((e & fmask) == fp[u]) {
+            const int row = (int)(e & t.rmask);
+            if (b0[row] == k0[u] && (!TWO || b1[row] == k1[u])) {
+              r[u] = row;
+              break;
+            }
+          }
+          s = uh_next(s, t.cap);
         }
       }
-      s = (s + 1) & mask;
     }
-    partner[i] = r;
-    c += r >= 0;
+#pragma unroll
+    for (int u = 0; u < UH_U; ++u) {
+      const long long i = base + (kk + u) * CT + threadIdx.x;
+      if (i < n) {
+        partner[i] = r[u];
+        c += r[u] >= 0;
+      }
+    }
   }
   __shared__ int red[CT / 32];
   for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(FULL, c, o);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
   __syncthreads();
   if (threadIdx.x == 0) {
-    int t = 0;
-    for (int q = 0; q < CT / 32; ++q) t += red[q];
-    bcnt[blockIdx.x] = t;
+    int s = 0;
+    for (int q = 0; q < CT / 32; ++q) s += red[q];
+    bcnt[blockIdx.x] = s;
   }
 }
 
@@ -299,7 +374,7 @@ __global__ void __launch_bounds__(T) k_expand(const long long* __restrict__ sort
 }
 
 struct UhLayout {
-  unsigned long long* table;
+  UhTable table;
   int* partner;
   long long* bcnt;
   long long* total;
@@ -307,12 +382,66 @@ struct UhLayout {
 
 UhLayout uh_layout(Arena& a, long long nb, long long np) {
   UhLayout l{};
-  const uint64_t cap = pow2_at_least((uint64_t)std::max<long long>(2 * nb, 2));
-  l.table = a.take<unsigned long long>(cap);
+  l.table.cap = (unsigned long long)std::max<long long>(2 * nb, 2);
+  int r = 1;
+  while (r < 31 && (1LL << r) - 1 < nb) ++r;  // nb <= 2^r - 1 (nb < 2^31)
+  l.table.rbits = r;
+  l.table.rmask = (1u << r) - 1;
+  l.table.slot = a.take<unsigned>(l.table.cap);
   l.partner = a.take<int>(std::max<long long>(np, 1));
   l.bcnt = a.take<long long>((np + CB - 1) / CB + 1);
   l.total = a.take<long long>(1);
   return l;
+}
+
+// Queues the table's reset, build and probe, and the scan of the probe
+// blocks' match counts (the total also into *count, a device address).
+int uh_queue(const UhLayout& l, const int64_t* build0, const int64_t* build1, int64_t nb,
+             const int64_t* probe0, const int64_t* probe1, int64_t np, int nkeys,
+             long long* count, cudaStream_t st) {
+  PF_CUDA(cudaMemsetAsync(l.table.slot, 0xff, l.table.cap * sizeof(unsigned), st));
+  const unsigned nblk = blocks_for(np, CB);
+  const long long* b0 = (const long long*)build0;
+  const long long* b1 = (const long long*)(nkeys == 2 ? build1 : build0);
+  const long long* p0 = (const long long*)probe0;
+  const long long* p1 = (const long long*)(nkeys == 2 ? probe1 : probe0);
+  if (nkeys == 2) {
+    {
+      PF_KERNEL("k_uh_build", st);
+      k_uh_build<true><<<blocks_for(nb, T), T, 0, st>>>(b0, b1, nb, l.table);
+    }
+    {
+      PF_KERNEL("k_uh_probe", st);
+      k_uh_probe<true><<<nblk, CT, 0, st>>>(b0, b1, p0, p1, np, l.table, l.partner, l.bcnt);
+    }
+  } else {
+    {
+      PF_KERNEL("k_uh_build", st);
+      k_uh_build<false><<<blocks_for(nb, T), T, 0, st>>>(b0, b1, nb, l.table);
+    }
+    {
+      PF_KERNEL("k_uh_probe", st);
+      k_uh_probe<false><<<nblk, CT, 0, st>>>(b0, b1, p0, p1, np, l.table, l.partner, l.bcnt);
+    }
+  }
+  PF_LAUNCH("k_uh_build/k_uh_probe");
+  {
+    PF_KERNEL("k_scan_counts", st);
+    k_scan_counts<<<1, 1024, 0, st>>>(l.bcnt, nblk, l.total, count);
+  }
+  PF_LAUNCH("k_scan_counts");
+  return PF_OK;
+}
+
+int uh_emit(const UhLayout& l, int64_t np, int64_t* build_idx, int64_t* probe_idx,
+            cudaStream_t st) {
+  {
+    PF_KERNEL("k_uh_emit", st);
+    k_uh_emit<<<blocks_for(np, CB), CT, 0, st>>>(l.partner, np, l.bcnt, (long long*)build_idx,
+                                                 (long long*)probe_idx);
+  }
+  PF_LAUNCH("k_uh_emit");
+  return PF_OK;
 }
 
 struct SaLayout {
@@ -371,47 +500,11 @@ extern "C" int pf_join_unique_hash(const int64_t* build0, const int64_t* build1,
   long long* host_dev = nullptr;
   if (int rc = host_alias(host_out, (void**)&host_dev)) return rc;
   host_out[1] = 0;
-  const uint64_t cap = pow2_at_least((uint64_t)std::max<long long>(2 * n_build, 2));
-  const int logcap = log2_exact(cap);
-  PF_CUDA(cudaMemsetAsync(l.table, 0xff, cap * sizeof(unsigned long long), st));
-  const unsigned nblk = blocks_for(n_probe, CB);
-  const long long* b0 = (const long long*)build0;
-  const long long* b1 = (const long long*)(nkeys == 2 ? build1 : build0);
-  const long long* p0 = (const long long*)probe0;
-  const long long* p1 = (const long long*)(nkeys == 2 ? probe1 : probe0);
-  if (nkeys == 2) {
-    {
-      PF_KERNEL("k_uh_build", st);
-      k_uh_build<true><<<blocks_for(n_build, T), T, 0, st>>>(b0, b1, n_build, l.table, logcap);
-    }
-    {
-      PF_KERNEL("k_uh_probe", st);
-      k_uh_probe<true><<<nblk, CT, 0, st>>>(b0, b1, p0, p1, n_probe, l.table, logcap, l.partner, l.bcnt);
-    }
-  } else {
-    {
-      PF_KERNEL("k_uh_build", st);
-      k_uh_build<false><<<blocks_for(n_build, T), T, 0, st>>>(b0, b1, n_build, l.table, logcap);
-    }
-    {
-      PF_KERNEL("k_uh_probe", st);
-      k_uh_probe<false><<<nblk, CT, 0, st>>>(b0, b1, p0, p1, n_probe, l.table, logcap, l.partner, l.bcnt);
-    }
-  }
-  PF_LAUNCH("k_uh_build/k_uh_probe");
-  {
-    PF_KERNEL("k_scan_counts", st);
-    k_scan_counts<<<1, 1024, 0, st>>>(l.bcnt, nblk, l.total, host_dev);
-  }
-  PF_LAUNCH("k_scan_counts");
+  if (int rc = uh_queue(l, build0, build1, n_build, probe0, probe1, n_probe, nkeys, host_dev, st))
+    return rc;
   cudaEvent_t ev;
   if (int rc = record_event(st, &ev)) return rc;
-  {
-    PF_KERNEL("k_uh_emit", st);
-    k_uh_emit<<<nblk, CT, 0, st>>>(l.partner, n_probe, l.bcnt, (long long*)build_idx,
-                                   (long long*)probe_idx);
-  }
-  PF_LAUNCH("k_uh_emit");
+  if (int rc = uh_emit(l, n_probe, build_idx, probe_idx, st)) return rc;
   if (int rc = wait_event(ev)) return rc;
   return ok();
 }
@@ -620,7 +713,7 @@ extern "C" int pf_join_unique_hash_static(const int64_t* build0, const int64_t* 
   if (need.used > (size_t)PF_UH_STATIC_SCRATCH_BYTES)
     return fail(PF_EINVAL,
                 "join_unique_hash_static: %lld build x %lld probe rows need %zu bytes of "
-                "scratch, the static scratch holds %zu (e.g. up to 262144 build with "
+                "scratch, the static scratch holds %zu (e.g. up to 524288 build with "
                 "1048576 probe rows); use pf_join_unique_hash",
                 (long long)n_build, (long long)n_probe, need.used,
                 (size_t)PF_UH_STATIC_SCRATCH_BYTES);
@@ -628,48 +721,11 @@ extern "C" int pf_join_unique_hash_static(const int64_t* build0, const int64_t* 
   if (int rc = uh_static_scratch(&scratch)) return rc;
   Arena a(scratch, PF_UH_STATIC_SCRATCH_BYTES);
   UhLayout l = uh_layout(a, n_build, n_probe);
-  const uint64_t cap = pow2_at_least((uint64_t)std::max<long long>(2 * n_build, 2));
-  const int logcap = log2_exact(cap);
   // the table starts empty (all ones) every call; partners, block counts and
   // the total are written in full before they are read
-  PF_CUDA(cudaMemsetAsync(l.table, 0xff, cap * sizeof(unsigned long long), st));
-  const unsigned nblk = blocks_for(n_probe, CB);
-  const long long* b0 = (const long long*)build0;
-  const long long* b1 = (const long long*)(nkeys == 2 ? build1 : build0);
-  const long long* p0 = (const long long*)probe0;
-  const long long* p1 = (const long long*)(nkeys == 2 ? probe1 : probe0);
-  if (nkeys == 2) {
-    {
-      PF_KERNEL("k_uh_build", st);
-      k_uh_build<true><<<blocks_for(n_build, T), T, 0, st>>>(b0, b1, n_build, l.table, logcap);
-    }
-    {
-      PF_KERNEL("k_uh_probe", st);
-      k_uh_probe<true><<<nblk, CT, 0, st>>>(b0, b1, p0, p1, n_probe, l.table, logcap, l.partner,
-                                            l.bcnt);
-    }
-  } else {
-    {
-      PF_KERNEL("k_uh_build", st);
-      k_uh_build<false><<<blocks_for(n_build, T), T, 0, st>>>(b0, b1, n_build, l.table, logcap);
-    }
-    {
-      PF_KERNEL("k_uh_probe", st);
-      k_uh_probe<false><<<nblk, CT, 0, st>>>(b0, b1, p0, p1, n_probe, l.table, logcap,
-                                             l.partner, l.bcnt);
-    }
-  }
-  PF_LAUNCH("k_uh_build/k_uh_probe");
-  {
-    PF_KERNEL("k_scan_counts", st);
-    k_scan_counts<<<1, 1024, 0, st>>>(l.bcnt, nblk, l.total, (long long*)match_count);
-  }
-  PF_LAUNCH("k_scan_counts");
-  {
-    PF_KERNEL("k_uh_emit", st);
-    k_uh_emit<<<nblk, CT, 0, st>>>(l.partner, n_probe, l.bcnt, (long long*)build_idx,
-                                   (long long*)probe_idx);
-  }
-  PF_LAUNCH("k_uh_emit");
+  if (int rc = uh_queue(l, build0, build1, n_build, probe0, probe1, n_probe, nkeys,
+                        (long long*)match_count, st))
+    return rc;
+  if (int rc = uh_emit(l, n_probe, build_idx, probe_idx, st)) return rc;
   return ok();
 }

@@ -173,6 +173,25 @@ def test_unique_hash_large_vs_oracle():
     assert np.array_equal(pi.cpu().numpy(), opi) and np.array_equal(bi.cpu().numpy(), obi)
 
 
+def test_unique_hash_chains_of_one_fingerprint():
+    """Build keys whose hashes differ only in bits 30-35: one home slot and one
+    fingerprint for all of them (the table keeps the hash's low bits beside
+    the row), so a probe walks a chain of fingerprint matches and checks each
+    candidate's key; probe keys made the same way but absent walk it to the
+    end and miss."""
+    from tests.test_aggregate_gpu import _unmix64
+    h0 = 0x5DEECE66D1234567
+    chain = [_unmix64((h0 + (j << 30)) & ((1 << 64) - 1)) for j in range(80)]
+    rest = (torch.randperm(1 << 20, generator=torch.Generator().manual_seed(5))[:1000] + 7).tolist()
+    bk = _cuda(chain[:64] + [k for k in rest if k not in set(chain)])
+    probe = chain[::-1] + rest[::3] + chain[60:70] + [k + (1 << 40) for k in rest[:50]]
+    pk = _cuda(probe)
+    bi, pi = join_core.unique_hash_pairs([bk], [pk])
+    obi, opi = oracle.join_unique([bk.cpu().numpy()], [pk.cpu().numpy()])
+    assert np.array_equal(pi.cpu().numpy(), opi) and np.array_equal(bi.cpu().numpy(), obi)
+    assert torch.equal(pk[pi], bk[bi]) and pi.numel() == 64 + len(rest[::3]) + 4
+
+
 def test_empty_sides():
     e = torch.empty(0, dtype=torch.int64, device="cuda")
     k = _cuda([1, 2])

@@ -55,7 +55,7 @@ def test_static_scratch_matches_workspace_path_twice_in_a_row(nkeys):
     # the largest sizes the scratch holds, then a small call on other keys
     # right after it on the same stream: the second call must not see the
     # first call's table
-    cases = [(11, 262144, 1048576), (12, 1000, 5000)]
+    cases = [(11, 524288, 1048576), (12, 1000, 5000)]
     inputs = [_inputs(seed, nb, npr, nkeys) for seed, nb, npr in cases]
     wants = [_with_workspace(b, p, nkeys) for b, p in inputs]
     outs = []
@@ -78,7 +78,7 @@ def test_static_scratch_matches_workspace_path_twice_in_a_row(nkeys):
 def test_static_scratch_refuses_sizes_past_its_limit():
     L = _native.lib()
     cnt = torch.empty(1, dtype=torch.int64, device="cuda")
-    for nb, npr in [(524289, 1000), (1000, 4 * 1048576)]:
+    for nb, npr in [(1100000, 1000), (1000, 4 * 1048576)]:
         # buffers of the sizes claimed, though the call must refuse them
         bk = torch.zeros(nb, dtype=torch.int64, device="cuda")
         pk = torch.zeros(npr, dtype=torch.int64, device="cuda")
