@@ -14,9 +14,9 @@
 //
 // A radix pass: k_rs_hist counts each 4096-key tile's digits; an exclusive
 // scan over [digit][tile] gives every (digit, tile) run's output start;
-// k_rs_scatter ranks each tile's keys stably - 256 keys a round, a key's rank
-// among its warp's equal digits from eight ballots, the warps' counts
-// prefixed per digit in shared memory - and writes them.
+// k_rs_scatter ranks each tile's keys stably - a key's rank among its warp's
+// equal digits from __match_any_sync, the warps' counts prefixed per digit in
+// shared memory - and writes them through a staged copy of the tile.
 #include <algorithm>
 #include <climits>
 #include <map>
@@ -29,7 +29,6 @@ namespace {
 constexpr int RT = 256;
 constexpr int RITEMS = 16;
 constexpr int RTILE = RT * RITEMS;
-constexpr int RW = RT / 32;
 
 __global__ void k_minmax_init(long long* mm) {
   mm[0] = LLONG_MAX;
@@ -66,33 +65,44 @@ __global__ void __launch_bounds__(RT) k_rs_hist(const long long* __restrict__ ke
   h[threadIdx.x] = 0;
   __syncthreads();
   const long long t0 = (long long)blockIdx.x * RTILE;
-#pragma unroll 4
+  long long kv[RITEMS];
+#pragma unroll
   for (int k = 0; k < RITEMS; ++k) {
     const long long i = t0 + k * RT + threadIdx.x;
-    if (i < n) atomicAdd(&h[digit_of(keys[i], kmin, shift)], 1);
+    kv[k] = i < n ? keys[i] : 0;
   }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < RITEMS; ++k)
+    if (t0 + k * RT + threadIdx.x < n) atomicAdd(&h[digit_of(kv[k], kmin, shift)], 1);
   __syncthreads();
   hist[(long long)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
 }
 
-// Each warp takes a contiguous 512-key segment of the tile (16 keys a lane,
-// in registers) and counts its digits; the counts give every digit's place
-// in the tile (digit order) and each warp's place inside it; each warp puts
-// its keys there in order - a round of 32 keys at a time, a key's place its
-// digit's running count in the warp plus its rank among the round's equal
-// digits (eight ballots) - in shared memory; then the block writes the tile
-// out digit run by digit run, consecutive threads on consecutive rows.
+// 512 threads take a tile, each warp a contiguous 256-key segment (8 keys a
+// lane, item k of lane l at w*256 + k*32 + l).  A key's place among its
+// warp's equal digits comes from __match_any_sync, item by item; the warps'
+// digit counts give every digit's run in the tile (digit order) and each
+// warp's place inside it.  The keys are staged at their places in shared
+// memory and written out digit run by digit run, consecutive threads on
+// consecutive rows; then the values the same way through the same buffer
+// (their loads issued before the keys' write-out).
+constexpr int ST = 512;
+constexpr int SI = RTILE / ST;  // keys a thread
+constexpr int SW = ST / 32;
+constexpr int SSEG = SI * 32;   // keys a warp
+static_assert(ST >= 256, "a thread a digit");
+
 struct ScatterSmem {
-  long long sk[RTILE];
-  long long sv[RTILE];
-  int wcnt[RW][256];   // the warp's digit counts, then its running place
-  int wloc[RW][256];   // the warp's first place per digit in the tile
-  int tstart[256];     // the digit's first place in the tile
+  long long stage[RTILE];
+  int wh[SW][256];  // the warp's digit counts, then its place in the digit's run
+  int tstart[256];  // the digit's first place in the tile
   long long gbase[256];
-  int wsum[RW];
+  unsigned char sdig[RTILE];
+  int wsum[SW];
 };
 
-__global__ void __launch_bounds__(RT, 2) k_rs_scatter(const long long* __restrict__ kin,
+__global__ void __launch_bounds__(ST) k_rs_scatter(const long long* __restrict__ kin,
                                                    const long long* __restrict__ vin, long long n,
                                                    long long kmin, int shift, int ntiles,
                                                    const long long* __restrict__ offsets,
@@ -101,82 +111,93 @@ __global__ void __launch_bounds__(RT, 2) k_rs_scatter(const long long* __restric
   extern __shared__ __align__(16) unsigned char rs_smem[];
   ScatterSmem& S = *reinterpret_cast<ScatterSmem*>(rs_smem);
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-#pragma unroll
-  for (int q = 0; q < RW; ++q) S.wcnt[q][tid] = 0;
-  S.gbase[tid] = offsets[(long long)tid * ntiles + blockIdx.x];
-  __syncthreads();
-  constexpr int SEG = RTILE / RW;  // 512 keys a warp
+  for (int x = tid; x < SW * 256; x += ST) (&S.wh[0][0])[x] = 0;
   const long long t0 = (long long)blockIdx.x * RTILE;
-  const long long s0 = t0 + (long long)w * SEG;
-  long long key[RITEMS], val[RITEMS];
-  int dig[RITEMS];
+  const long long s0 = t0 + (long long)w * SSEG + lane;
+  long long key[SI];
+  int dig[SI];
 #pragma unroll
-  for (int k = 0; k < RITEMS; ++k) {
-    const long long i = s0 + k * 32 + lane;
-    const bool valid = i < n;
-    key[k] = valid ? kin[i] : 0;
-    val[k] = valid ? (vin ? vin[i] : i) : 0;
-    dig[k] = valid ? digit_of(key[k], kmin, shift) : -1;
-    if (valid) atomicAdd(&S.wcnt[w][dig[k]], 1);
-  }
+  for (int k = 0; k < SI; ++k) key[k] = s0 + k * 32 < n ? kin[s0 + k * 32] : 0;
+  const long long goff = tid < 256 ? offsets[(long long)tid * ntiles + blockIdx.x] : 0;
+#pragma unroll
+  for (int k = 0; k < SI; ++k) dig[k] = s0 + k * 32 < n ? digit_of(key[k], kmin, shift) : -1;
   __syncthreads();
-  // thread tid owns digit tid: its total, the tile's exclusive scan over
-  // digits, then each warp's place
-  int tot = 0;
-#pragma unroll
-  for (int q = 0; q < RW; ++q) tot += S.wcnt[q][tid];
-  int incl = tot;
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(FULL, incl, o);
-    if (lane >= o) incl += y;
-  }
-  if (lane == 31) S.wsum[w] = incl;
-  __syncthreads();
-  int pre = 0;
-#pragma unroll
-  for (int q = 0; q < RW; ++q) pre += q < w ? S.wsum[q] : 0;
-  const int start = pre + incl - tot;
-  S.tstart[tid] = start;
+  int sk[SI];
   {
-    int b = start;
+    const unsigned lt = lanemask_lt();
 #pragma unroll
-    for (int q = 0; q < RW; ++q) {
-      S.wloc[q][tid] = b;
-      b += S.wcnt[q][tid];
-      S.wcnt[q][tid] = 0;
+    for (int k = 0; k < SI; ++k) {
+      const unsigned peers = __match_any_sync(FULL, dig[k]);
+      const int before = __popc(peers & lt);
+      const int base = dig[k] >= 0 ? S.wh[w][dig[k]] : 0;
+      __syncwarp();
+      if (dig[k] >= 0 && before == 0) S.wh[w][dig[k]] = base + __popc(peers);
+      __syncwarp();
+      sk[k] = base + before;
     }
   }
   __syncthreads();
-  const unsigned lt = (1u << lane) - 1u;
+  // thread d < 256: digit d's warps' places and its count in the tile, then
+  // the tile's exclusive scan over the digits
+  {
+    int tot = 0;
+    if (tid < 256) {
 #pragma unroll
-  for (int k = 0; k < RITEMS; ++k) {
-    const int d = dig[k];
-    const bool valid = d >= 0;
-    unsigned peers = __ballot_sync(FULL, valid);
+      for (int q = 0; q < SW; ++q) {
+        const int t = S.wh[q][tid];
+        S.wh[q][tid] = tot;
+        tot += t;
+      }
+    }
+    int incl = tot;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) S.wsum[w] = incl;
+    __syncthreads();
+    if (tid < 256) {
+      int pre = 0;
 #pragma unroll
-    for (int b = 0; b < 8; ++b) {
-      const unsigned bb = __ballot_sync(FULL, (d >> b) & 1);
-      peers &= ((d >> b) & 1) ? bb : ~bb;
+      for (int q = 0; q < 256 / 32; ++q) pre += q < w ? S.wsum[q] : 0;
+      const int start = pre + incl - tot;
+      S.tstart[tid] = start;
+      S.gbase[tid] = goff - start;
     }
-    const int before = __popc(peers & lt);
-    const int run = valid ? S.wcnt[w][d] : 0;
-    __syncwarp();
-    if (valid) {
-      const int loc = S.wloc[w][d] + run + before;
-      S.sk[loc] = key[k];
-      S.sv[loc] = val[k];
-      if (before == 0) S.wcnt[w][d] = run + __popc(peers);
+    __syncthreads();
+  }
+  int slot[SI];
+#pragma unroll
+  for (int k = 0; k < SI; ++k) {
+    slot[k] = 0;
+    if (dig[k] >= 0) {
+      slot[k] = S.tstart[dig[k]] + S.wh[w][dig[k]] + sk[k];
+      S.sdig[slot[k]] = (unsigned char)dig[k];
+      S.stage[slot[k]] = key[k];
     }
-    __syncwarp();
   }
   __syncthreads();
+  long long val[SI];
+#pragma unroll
+  for (int k = 0; k < SI; ++k) {
+    const long long i = s0 + k * 32;
+    val[k] = i < n ? (vin ? vin[i] : i) : 0;
+  }
   const int cnt = (int)min((long long)RTILE, n - t0);
-  for (int e = tid; e < cnt; e += RT) {
-    const long long kk = S.sk[e];
-    const int d = digit_of(kk, kmin, shift);
-    const long long pos = S.gbase[d] + (e - S.tstart[d]);
-    kout[pos] = kk;
-    vout[pos] = S.sv[e];
+#pragma unroll
+  for (int t = 0; t < SI; ++t) {
+    const int e = t * ST + tid;
+    if (e < cnt) kout[S.gbase[S.sdig[e]] + e] = S.stage[e];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < SI; ++k)
+    if (dig[k] >= 0) S.stage[slot[k]] = val[k];
+  __syncthreads();
+#pragma unroll
+  for (int t = 0; t < SI; ++t) {
+    const int e = t * ST + tid;
+    if (e < cnt) vout[S.gbase[S.sdig[e]] + e] = S.stage[e];
   }
 }
 
@@ -274,7 +295,7 @@ int sort_pairs(const long long* kin, const long long* vin, long long n, long lon
     if (int rc = scan_i64(l.hist, l.offs, 256LL * ntiles, false, nullptr, l.scratch, st)) return rc;
     {
       PF_KERNEL("k_rs_scatter", st);
-      k_rs_scatter<<<ntiles, RT, sizeof(ScatterSmem), st>>>(sk, sv, n, mm[0], 8 * p, ntiles,
+      k_rs_scatter<<<ntiles, ST, sizeof(ScatterSmem), st>>>(sk, sv, n, mm[0], 8 * p, ntiles,
                                                             l.offs, dk, dv);
     }
     PF_LAUNCH("k_rs_scatter");
