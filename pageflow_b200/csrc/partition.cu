@@ -632,7 +632,7 @@ __device__ __forceinline__ void plain_write(const PlainSmem& S, unsigned char* o
 }
 
 #ifndef PF_PART_PLAIN_MINB
-#define PF_PART_PLAIN_MINB 1
+#define PF_PART_PLAIN_MINB 2  // two blocks a SM: at most 64 registers a thread
 #endif
 __global__ void __launch_bounds__(PT, PF_PART_PLAIN_MINB) k_scatter_plain(Params p) {
   if (failed(p)) return;

@@ -102,7 +102,7 @@ struct ScatterSmem {
   int wsum[SW];
 };
 
-__global__ void __launch_bounds__(ST) k_rs_scatter(const long long* __restrict__ kin,
+__global__ void __launch_bounds__(ST, 2) k_rs_scatter(const long long* __restrict__ kin,
                                                    const long long* __restrict__ vin, long long n,
                                                    long long kmin, int shift, int ntiles,
                                                    const long long* __restrict__ offsets,
