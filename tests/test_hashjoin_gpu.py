@@ -214,6 +214,34 @@ def test_gather_matches_index_with_null(dtype):
     assert torch.equal(sel[1].cpu(), src[idx.clamp(min=0), 0])
 
 
+@pytest.mark.parametrize("ncols", [1, 2, 3, 4])
+def test_gather_one_word_rows_with_nulls_and_a_ragged_tail(ncols):
+    """Columns whose rows are one 1-16 byte word take the batched kernel:
+    nulls, an out-of-range index and a row count that is not a multiple of
+    the rows a block takes."""
+    g = torch.Generator().manual_seed(17 + ncols)
+    n_src, n = 1000, 3 * 1024 + 37
+    pool = [torch.randint(-(1 << 40), 1 << 40, (n_src,), generator=g),
+            torch.randint(-(1 << 30), 1 << 30, (n_src,), generator=g, dtype=torch.int32),
+            torch.randint(-100, 100, (n_src,), generator=g).to(torch.int16),
+            torch.randint(-100, 100, (n_src,), generator=g).to(torch.int8),
+            torch.randint(-(1 << 40), 1 << 40, (n_src, 2), generator=g),
+            torch.randn(n_src, generator=g, dtype=torch.float64)]
+    cols = [pool[(ncols + k) % len(pool)] for k in range(ncols)]
+    idx = torch.randint(0, n_src, (n,), generator=g)
+    idx[::5] = -64
+    idx[7] = n_src
+    out = gather.index_with_null_many([c.cuda() for c in cols], idx.cuda())
+    bad = (idx == n_src) | (idx == -64)
+    for o, c in zip(out, cols):
+        want = c[idx.clamp(0, n_src - 1)]
+        want[bad] = torch.full((1,), -64, dtype=c.dtype)
+        assert torch.equal(o.cpu(), want)
+    sel = gather.index_select_many([c.cuda() for c in cols], idx.clamp(0, n_src - 1).cuda())
+    for o, c in zip(sel, cols):
+        assert torch.equal(o.cpu(), c[idx.clamp(0, n_src - 1)])
+
+
 def test_gather_counts_out_of_range_and_reads_nothing_outside():
     src = torch.arange(100, dtype=torch.int64, device="cuda")
     idx = torch.tensor([0, 99, 100, -1, 5, 1 << 40], dtype=torch.int64, device="cuda")
