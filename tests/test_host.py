@@ -53,7 +53,8 @@ def test_workspace_sizes_are_host_arithmetic():
     a = L.pf_partition_sort_workspace(1 << 20, 1 << 20, 64, 0, 0)
     b = L.pf_partition_sort_workspace(1 << 24, 1 << 24, 512, 1, 1)
     assert 0 < a < b
-    assert L.pf_join_unique_hash_workspace(1000, 2000) >= 2048 * 8 + 2000 * 4
+    # a table of 2 x n_build 4-byte slots and a 4-byte partner a probe row
+    assert L.pf_join_unique_hash_workspace(1000, 2000) >= 2 * 1000 * 4 + 2000 * 4
     assert L.pf_join_aggregate_workspace(1000, 4000, 1, 25) >= 1000 * 12 + 4000 * 16
     assert L.pf_join_aggregate_pick_b(250_000, 1_000_000) == 1
     assert 256 <= L.pf_join_aggregate_pick_b(150_000_000, 600_000_000) <= 4096
