@@ -175,7 +175,7 @@ def test_static_scratch_join_refuses_sizes_before_any_device_work():
     from pageflow_b200 import _native
     L = _native.lib()
     fake = ctypes.c_void_p(256)
-    for nb, npr in [(262144 + 1, 1048576), (524289, 10), (10, 4 * 1048576)]:
+    for nb, npr in [(540000, 1048576), (1100000, 10), (10, 4 * 1048576)]:
         rc = L.pf_join_unique_hash_static(fake, None, nb, fake, None, npr, 1, fake, fake, fake,
                                           None)
         assert rc == _native.PF_EINVAL
