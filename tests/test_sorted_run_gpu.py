@@ -20,11 +20,11 @@ I64 = np.iinfo(np.int64)
 
 
 @pytest.mark.parametrize("case", ["full", "small", "dups", "one_value", "single", "empty",
-                                  "negative", "large"])
+                                  "negative", "large", "tiny_full"])
 def test_radix_sort_is_a_stable_sort(case):
-    rng = np.random.default_rng(hash(case) % 1000)
-    n = {"single": 1, "empty": 0, "large": 3_000_000}.get(case, 50_000)
-    if case == "full":
+    rng = np.random.default_rng(sum(map(ord, case)))
+    n = {"single": 1, "empty": 0, "large": 3_000_000, "tiny_full": 1000}.get(case, 50_000)
+    if case in ("full", "tiny_full"):
         k = rng.integers(I64.min, I64.max, n, dtype=np.int64)
     elif case in ("small", "large"):
         k = rng.integers(-300, 300, n).astype(np.int64)
