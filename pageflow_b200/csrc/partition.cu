@@ -619,15 +619,17 @@ __device__ __forceinline__ void plain_stage(PlainSmem& S, const int (&slot)[PITE
     if (valid[k]) stage[slot[k]] = (T)v[k];
 }
 
+// eb[t]: the bucket of staged row t*PT + tid (read once for all columns)
 template <typename T>
 __device__ __forceinline__ void plain_write(const PlainSmem& S, unsigned char* out_,
-                                            const long long* gbc, int tvalid) {
+                                            const long long* gbc, int tvalid,
+                                            const int (&eb)[PITEMS]) {
   const T* stage = reinterpret_cast<const T*>(S.stage);
   T* out = reinterpret_cast<T*>(out_);
 #pragma unroll
   for (int t = 0; t < PITEMS; ++t) {
     const int e = t * PT + threadIdx.x;
-    if (e < tvalid) out[gbc[S.sbk[e]] + e] = stage[e];
+    if (e < tvalid) out[gbc[eb[t]] + e] = stage[e];
   }
 }
 
@@ -732,6 +734,12 @@ __global__ void __launch_bounds__(PT, PF_PART_PLAIN_MINB) k_scatter_plain(Params
   }
   __syncthreads();
   const int tvalid = S.tvalid;
+  int eb[PITEMS];
+#pragma unroll
+  for (int t = 0; t < PITEMS; ++t) {
+    const int e = t * PT + tid;
+    eb[t] = e < tvalid ? S.sbk[e] : 0;
+  }
   for (int c = 0; c < p.c.ncols; ++c) {
     const long long* gbc = S.gb[p.c.cls[c]];
     const int rb = p.c.rb[c];
@@ -745,10 +753,10 @@ __global__ void __launch_bounds__(PT, PF_PART_PLAIN_MINB) k_scatter_plain(Params
     __syncthreads();
     if (c + 1 < p.c.ncols) plain_load(p, c + 1, t0, valid, v);
     switch (rb) {
-      case 8: plain_write<unsigned long long>(S, out, gbc, tvalid); break;
-      case 4: plain_write<unsigned>(S, out, gbc, tvalid); break;
-      case 2: plain_write<unsigned short>(S, out, gbc, tvalid); break;
-      default: plain_write<unsigned char>(S, out, gbc, tvalid); break;
+      case 8: plain_write<unsigned long long>(S, out, gbc, tvalid, eb); break;
+      case 4: plain_write<unsigned>(S, out, gbc, tvalid, eb); break;
+      case 2: plain_write<unsigned short>(S, out, gbc, tvalid, eb); break;
+      default: plain_write<unsigned char>(S, out, gbc, tvalid, eb); break;
     }
     __syncthreads();
   }
@@ -756,7 +764,7 @@ __global__ void __launch_bounds__(PT, PF_PART_PLAIN_MINB) k_scatter_plain(Params
 #pragma unroll
   for (int t = 0; t < PITEMS; ++t) {
     const int e = t * PT + tid;
-    if (e < tvalid) p.gout[gbg[S.sbk[e]] + e] = p.goff + t0 + S.srow[e];
+    if (e < tvalid) p.gout[gbg[eb[t]] + e] = p.goff + t0 + S.srow[e];
   }
 }
 
