@@ -41,13 +41,12 @@ def expand(sorted_ids: torch.Tensor, start: torch.Tensor,
 
 
 def unique_hash_peak_bytes(n_build: int, n_probe: int) -> int:
-    """Scratch of a ``unique_hash_pairs`` call: the table (8-byte slots, a
-    power of two at least twice the build rows), the partner and the two
-    probe-sized outputs."""
-    cap = 1
-    while cap < 2 * max(n_build, 1):
-        cap <<= 1
-    return cap * 8 + n_probe * (4 + 8 + 8)
+    """Scratch of a ``unique_hash_pairs`` call, the figure the join's dispatch
+    compares with its limit (reference operators/join_core.py:64-68): the
+    table (two 4-byte slots a build row), the 4-byte partner and the two
+    8-byte outputs of every probe row.  The library's workspace adds a few
+    bytes per 4096 probe rows for block counts."""
+    return 2 * n_build * 4 + n_probe * (4 + 8 + 8)
 
 
 def _validate_keys(build_keys: Sequence[torch.Tensor], probe_keys: Sequence[torch.Tensor]):

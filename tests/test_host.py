@@ -218,3 +218,15 @@ def test_bench_functions_name_only_defined_names():
                     and not hasattr(builtins, node.id)):
                 missing.append(f"{fn.name}:{node.lineno}:{node.id}")
     assert missing == []
+
+
+def test_unique_hash_dispatch_estimate_is_the_references():
+    # the join's dispatch compares the reference's scratch figure
+    # (operators/join_core.py:64-68) with its limit; the library's own
+    # workspace for the table and the partners fits in that figure's share
+    # of them plus the per-block counts
+    from pageflow_b200 import _native, join_core
+    assert join_core.unique_hash_peak_bytes(1000, 2000) == 2 * 1000 * 4 + 2000 * 20
+    nb, npr = 10**6, 4 * 10**6
+    ws = _native.lib().pf_join_unique_hash_workspace(nb, npr)
+    assert 2 * nb * 4 + npr * 4 <= ws <= 2 * nb * 4 + npr * 4 + 64 * 1024
