@@ -5,9 +5,9 @@
 # Python extension module `tqpkernels` that TQPlib/tqpkernels re-exports.
 # Test infrastructure only (GPU parity of the drop-in against the reference's
 # kernels, and the GPU baseline of the reference's path); the product never
-# loads it.  Usage: oracle/build_ref.sh [/path/to/PageFlow]
+# loads it.  Usage: oracle/build_ref.sh /path/to/PageFlow (or PAGEFLOW_REFERENCE)
 set -euo pipefail
-REF=${1:-/root/reference}
+REF=${1:-${PAGEFLOW_REFERENCE:?give the reference checkout as the first argument or in PAGEFLOW_REFERENCE}}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 SRC="$REF/operators/kernels"

@@ -246,4 +246,8 @@ def main(root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    import os
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PAGEFLOW_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_golden.py <reference checkout> (or set PAGEFLOW_REFERENCE)")
+    main(ref)

@@ -1,7 +1,7 @@
 """CPU tests of the host side: the C-ABI library loads and exports every
 function include/pageflow_b200.h declares (no GPU work is started), the
 argument checks that run before any kernel, the partition-count rule against
-the reference's own values, and the operator mirrors' validation."""
+the reference's own values, and the drop-in module's validation."""
 from __future__ import annotations
 
 import ctypes
@@ -98,19 +98,21 @@ def test_partition_count_rule_is_the_references():
 
 
 def test_bucket_limit_is_the_join_cap():
-    from pageflow_b200 import partition_sort, partitions, tqpkernels
-    assert partition_sort._B_MAX == partitions.JOIN_B_MAX == tqpkernels.BMAX
+    from pageflow_b200 import partitions, tqpkernels
+    assert partitions.JOIN_B_MAX == tqpkernels.BMAX
     h = (REPO / "include" / "pageflow_b200.h").read_text()
     assert re.search(r"#define PF_PART_B_MAX (\d+)", h).group(1) == str(partitions.JOIN_B_MAX)
 
 
 @pytest.mark.parametrize("case", ["five widths", "seven columns", "int32 key", "B=1024",
-                                  "B=24", "B=0"])
-def test_ticks_outside_the_limits_raise(case):
-    """The mirror's limits, checked before any kernel (CPU tensors suffice)."""
-    from pageflow_b200.partition_sort import partition
+                                  "B=24", "B=0", "host_out too short", "pageable host_out"])
+def test_drop_in_partition_refuses_bad_arguments_before_any_kernel(case):
+    """The drop-in's argument checks raise RuntimeError, as the reference's
+    TORCH_CHECKs do, before touching a device (CPU tensors suffice)."""
+    from pageflow_b200 import tqpkernels
     n = 1000
     key = torch.arange(n, dtype=torch.int64)
+    host = torch.empty(512 + 5, dtype=torch.int64, pin_memory=torch.cuda.is_available())
     cols, B = {
         "five widths": ([key, key.to(torch.int32), key.to(torch.int16), key.to(torch.int8),
                          torch.zeros(n, 25, dtype=torch.uint8)], 32),
@@ -119,46 +121,29 @@ def test_ticks_outside_the_limits_raise(case):
         "B=1024": ([key], 1024),
         "B=24": ([key], 24),
         "B=0": ([key], 0),
+        "host_out too short": ([key], 32),
+        "pageable host_out": ([key], 32),
     }[case]
-    with pytest.raises(ValueError, match="outside the kernel's limits"):
-        partition(cols, 0, None, 0, B)
+    if case == "host_out too short":
+        host = host[:10]
+    if case == "pageable host_out":
+        host = torch.empty(512 + 5, dtype=torch.int64)
+    with pytest.raises(RuntimeError):
+        tqpkernels.partition_sort(cols, [0] * len(cols), 0, None, n, 0, B, False, host)
 
 
-def test_raw_columns_without_the_count_raise():
-    from pageflow_b200.partition_sort import partition
-    key = torch.arange(100, dtype=torch.int64)
-    mask = torch.ones(100, dtype=torch.bool)
-    with pytest.raises(ValueError, match="need the mask's kept rows"):
-        partition([key], 0, mask, 0, 16)
-
-
-def test_a_count_the_compacted_rows_contradict_raises():
-    from pageflow_b200.partition_sort import partition
-    key = torch.arange(50, dtype=torch.int64)
-    mask = torch.zeros(100, dtype=torch.bool)
-    mask[::2] = True
-    with pytest.raises(RuntimeError, match="compacted columns hold"):
-        partition([key], 0, mask, 0, 32, n_valid=51)
-
-
-def test_join_core_validation_runs_before_the_kernel():
-    from pageflow_b200 import join_core
+def test_drop_in_join_cores_refuse_bad_arguments_before_any_kernel():
+    from pageflow_b200 import tqpkernels
     k = torch.arange(4, dtype=torch.int64)
-    with pytest.raises(ValueError, match="1-D CUDA int64"):
-        join_core.unique_hash_pairs([k], [k])
-    with pytest.raises(ValueError, match="one or two"):
-        join_core.unique_hash_pairs([k, k, k], [k, k, k])
-
-
-def test_padded_layout_matches_the_oracle():
-    import oracle
-    from pageflow_b200.partition_sort import aligned_partition_layout
-    counts = [0, 5, 130, 1, 0, 64]
-    for rb in (1, 4, 8, 25):
-        unit = rb * 512 // __import__("math").gcd(rb, 512)
-        _, starts_b, total = aligned_partition_layout(counts, rb, unit)
-        starts, total2 = oracle.padded_layout(counts, rb)
-        assert [s // rb for s in starts_b] == starts and total == total2
+    host = torch.empty(2, dtype=torch.int64)
+    with pytest.raises(RuntimeError, match="one or two"):
+        tqpkernels.join_unique_hash([k, k, k], [k, k, k], host)
+    with pytest.raises(RuntimeError):
+        tqpkernels.join_unique_hash([k], [k], host)
+    with pytest.raises(RuntimeError):
+        tqpkernels.join_semi_anti(k, k, None, None, 0, False, host)
+    with pytest.raises(RuntimeError):
+        tqpkernels.join_expand(k, k, k, host)
 
 
 def test_slab_rejects_bad_specs_on_the_host():
@@ -220,13 +205,12 @@ def test_bench_functions_name_only_defined_names():
     assert missing == []
 
 
-def test_unique_hash_dispatch_estimate_is_the_references():
-    # the join's dispatch compares the reference's scratch figure
+def test_unique_hash_workspace_fits_the_references_scratch_figure():
+    # the reference's dispatch compares 2 * n_build * 4 + n_probe * 20 bytes
     # (operators/join_core.py:64-68) with its limit; the library's own
-    # workspace for the table and the partners fits in that figure's share
-    # of them plus the per-block counts
-    from pageflow_b200 import _native, join_core
-    assert join_core.unique_hash_peak_bytes(1000, 2000) == 2 * 1000 * 4 + 2000 * 20
+    # workspace for the table and the partners fits in that figure's share of
+    # them plus the per-block counts
+    from pageflow_b200 import _native
     nb, npr = 10**6, 4 * 10**6
     ws = _native.lib().pf_join_unique_hash_workspace(nb, npr)
     assert 2 * nb * 4 + npr * 4 <= ws <= 2 * nb * 4 + npr * 4 + 64 * 1024
