@@ -235,8 +235,16 @@ int pf_slab_finish(const uint8_t* occupied, int64_t key_min, int64_t capacity, i
  * or nonzero when a kernel gave up a bounded wait for its bulk copies; the
  * outputs are then not valid), build rows whose group is out of range (their
  * matches are not aggregated), and the number of build rows no table slot
- * took (0 on success).  Waits once, for the bucket counts that plan the
- * rounds; the rest stays queued.
+ * took (0 on success).
+ *
+ * The default (shared-memory) path counts no rows before it scatters: each
+ * bucket of the first radix pass, and each sub-bucket of the second, owns a
+ * region sized for its expected rows plus seven standard deviations, and a
+ * pass whose region would overflow (skewed keys) is run again after counting
+ * its rows exactly.  Waits for the first pass's bucket ends (they plan the
+ * second pass) and, unless the second pass was counted, for its overflow
+ * word at the end; with PF_JOIN_PATH=rounds it waits once, for the bucket
+ * counts that plan the rounds, and the rest stays queued.
  */
 size_t pf_join_aggregate_workspace(int64_t n_build, int64_t n_probe, int B, int64_t n_groups);
 int pf_join_aggregate(const int64_t* build_key, const int32_t* build_group, int64_t n_build,
@@ -246,6 +254,13 @@ int pf_join_aggregate(const int64_t* build_key, const int32_t* build_group, int6
                       int64_t* stats_out, void* workspace, size_t workspace_bytes, void* stream);
 /* The fan-out the autotuner seeds pf_join_aggregate with for these sizes. */
 int pf_join_aggregate_pick_b(int64_t n_build, int64_t n_probe);
+/*
+ * Which passes the calling thread's last pf_join_aggregate counted before it
+ * scattered: bit 0 the first radix pass, bit 1 the second (both taken again
+ * after a region overflowed, or forced with PF_COUNTED=1).  No counterpart in
+ * the reference, whose partition kernel always counts first.
+ */
+int pf_join_aggregate_counted_passes(void);
 /*
  * The groups a dense (sum, count) slab holds, ascending: keys_out[j] =
  * group_min + g, sums_out[j] = sum[g], counts_out[j] = count[g] for every g

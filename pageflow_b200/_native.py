@@ -61,6 +61,7 @@ _SIGS = {
     "pf_join_aggregate": (_int, [_vp, _vp, _i64, _vp, _vp, _vp, _i64, _i64, _int,
                                  _i64, _i64, _vp, _vp, _vp, _vp, _sz, _vp]),
     "pf_join_aggregate_pick_b": (_int, [_i64, _i64]),
+    "pf_join_aggregate_counted_passes": (_int, []),
     "pf_groups_finish_workspace": (_sz, [_i64]),
     "pf_groups_finish": (_int, [_vp, _vp, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _sz,
                                 _vp]),

@@ -40,7 +40,9 @@
 // sub-partitions.
 #include <algorithm>
 #include <climits>
+#include <cmath>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "scan.cuh"
@@ -72,6 +74,11 @@ constexpr long long ROUND_ROWS_DEFAULT = 1200 * 1024;
 // chooses at run time)
 #ifndef PF_JOIN_PATH_DEFAULT
 #define PF_JOIN_PATH_DEFAULT 1
+#endif
+// 1: the shared-memory join's table has fingerprinted 4-byte slots
+// (PF_SJ_FP=0|1 chooses at run time)
+#ifndef PF_SJ_FP_DEFAULT
+#define PF_SJ_FP_DEFAULT 0
 #endif
 
 struct Slot {
@@ -762,20 +769,29 @@ __global__ void __launch_bounds__(PT2, PF_PROBE_MINB) k_fround(RoundArgs pa, Rou
 
 // ---- the shared-memory join: a second radix pass, then per sub-partition ----
 //
-// PF_JOIN_PATH=smem (or the default when it is the faster path): the first
-// scatter carries each key's mix64 hash in place of the key (a bijection:
-// equal keys, equal hashes), each partition is split again by the next
-// log2(B2) bits of the hash (k_p2_hist, k_p2_colsum, scan, k_p2_scatter), so
-// every sub-partition holds about SJ_TARGET build rows; then k_sjoin takes
+// PF_JOIN_PATH=smem (the default): the first scatter carries each key's mix64
+// hash in place of the key (a bijection: equal keys, equal hashes), each
+// partition is split again by the next log2(B2) bits of the hash, so every
+// sub-partition holds about SJ_TARGET build rows; then k_sjoin takes
 // sub-partitions from a counter: it puts the build rows into a shared-memory
-// table {hash, group offset, sum, count}, adds every matching probe row's
-// value and 1 into its build row's cell with shared-memory atomics, and
-// flushes each build row that matched into the group slab with one pair of
-// global REDs.  Per probe row no L2 operation at all; per build row one pair.
-// A sub-partition with more build rows than the table takes is joined in
-// table-sized chunks of its build rows, each chunk against all of its probe
-// rows.  The table marks a free slot with the hash INT64_MIN; the key whose
-// hash that is gets a cell of its own.
+// table {hash, sum, count}, adds every matching probe row's value and 1 into
+// its build row's cell with shared-memory atomics, and flushes each build row
+// that matched into the group slab with one pair of global REDs.  Per probe
+// row no L2 operation at all; per build row one pair.  A sub-partition with
+// more build rows than the table takes is joined in table-sized chunks of its
+// build rows, each chunk against all of its probe rows.  The table marks a
+// free slot with the hash INT64_MIN; the key whose hash that is gets a cell of
+// its own.
+//
+// Neither radix pass counts its rows first.  Each (sub-)bucket owns a region
+// of the output sized for its expected rows plus seven standard deviations
+// (the hash spreads the keys of a side uniformly), and the scatter's cursor
+// claims run from the region's start.  A tile whose claim would cross its
+// region's end writes none of that bucket's rows and raises the overflow
+// word instead; the host sees it and runs that pass again with exact counts
+// (per-segment histograms and a scan: the counted passes).  Skewed keys, which
+// crowd one bucket, take that route; uniform ones never do.  The probe side
+// travels as 16-byte records {hash, value}: one load and one store a row.
 
 // One 1024-thread block a SM with 8192-row tiles: runs of 16 rows at 512
 // sub-buckets (measured against 512 threads x 4096 rows: 6.03 vs 6.79 ms for
@@ -791,7 +807,7 @@ __global__ void __launch_bounds__(PT2, PF_PROBE_MINB) k_fround(RoundArgs pa, Rou
 #endif
 constexpr int P2T = PF_P2T;
 constexpr int P2I = PF_P2I;
-constexpr int P2TILE = P2T * P2I;  // rows a pass-2 tile
+constexpr int P2TILE = P2T * P2I;  // rows a tile, at most
 // The first pass's probe side carries three input columns a row into its
 // registers: 6 rows a thread (6144-row tiles) keep it within 64 registers
 // without spilling (measured against 8 rows, which spilled: 5.50 vs 5.86 ms
@@ -800,15 +816,10 @@ constexpr int P2TILE = P2T * P2I;  // rows a pass-2 tile
 #define PF_P2_RI2 6
 #endif
 constexpr int P2RI2 = PF_P2_RI2;
-// 1: the shared-memory path's first pass through the tile scatter when
-// B <= P2BINS (PF_FIRST_TILE=0|1 chooses at run time)
-#ifndef PF_FIRST_TILE
-#define PF_FIRST_TILE 1
-#endif
 constexpr int P2MAXLOG = 10;       // sub-buckets a partition splits into, log2, at most
 constexpr int P2BINS = 1 << P2MAXLOG;
-constexpr int P2BPT = P2BINS / P2T;  // sub-buckets a thread scans
-static_assert(P2BINS % P2T == 0 && P2BPT >= 1, "whole sub-buckets a thread in the tile scan");
+constexpr int P1BINS = FB_MAX;     // the first pass's buckets, at most
+static_assert(P2BINS % P2T == 0 && P1BINS % P2T == 0, "whole bins a thread in the tile scan");
 // Three 384-thread blocks a SM, each with a 3072-slot table (63 KB of shared
 // memory: hash, two-word sum, count; no group offsets), measured against two
 // 512-thread blocks with 4096-slot tables and stored offsets: 4.72 vs 5.43 ms
@@ -836,11 +847,6 @@ constexpr int SJT = PF_SJT;       // threads of the join
 constexpr int SJ_TS = PF_SJ_TS;                // table slots
 constexpr bool SJ_POW2 = (SJ_TS & (SJ_TS - 1)) == 0;
 static_assert(!SJ_POW2 || SJ_TS == (1 << PF_SJ_LOGTS), "a power-of-two table is 2^PF_SJ_LOGTS slots");
-// 1: the join's table keeps no group offsets; the flush reads each matched
-// build row's group again (the row was read moments before, from L2)
-#ifndef PF_SJ_NOGOFF
-#define PF_SJ_NOGOFF 1
-#endif
 #ifndef PF_SJ_CAP
 #define PF_SJ_CAP (SJ_TS / 2)
 #endif
@@ -856,11 +862,18 @@ constexpr int SJ_BU = SJ_CAP / SJT;            // build rows a thread takes per 
 static_assert(SJ_CAP % SJT == 0, "whole build rounds");
 static_assert(SJ_TS < 0xffff, "slots fit the 16-bit slot index");
 
-// Pass 2 works on segments: runs of at most P2SEG rows inside one partition
-// (segment (p, j) is rows [start_p + j * P2SEG, min(start_p + (j + 1) * P2SEG,
-// end_p))), so a segment's rows share their partition and its 2^logB2
-// sub-buckets.
+// The counted second pass works on segments: runs of at most P2SEG rows
+// inside one partition (segment (p, j) is rows [start_p + j * P2SEG,
+// min(start_p + (j + 1) * P2SEG, end_p))), so a segment's rows share their
+// partition and its 2^logB2 sub-buckets.
 constexpr long long P2SEG = 16LL * P2TILE;
+
+// Rows a (sub-)bucket's region holds for `mean` expected rows: seven
+// standard deviations over the mean (the count is binomial, its deviation
+// below sqrt(mean)) and a few rows more.
+inline long long region_rows(double mean) {
+  return (long long)std::ceil(mean + 7.0 * std::sqrt(mean)) + 32;
+}
 
 struct SegArgs {
   const int2* seg;          // (partition, index in the partition)
@@ -879,9 +892,23 @@ __device__ __forceinline__ void seg_range(const SegArgs& g, int sg, long long& l
   base = (long long)d.x << g.logB2;
 }
 
+// A staged row: key (hash) and value in one 16-byte record; the probe side's
+// partitioned rows are stored in HBM in the same form.
+struct alignas(16) P2Row {
+  long long k;
+  long long v;
+};
+
+__device__ __forceinline__ P2Row stream_ld_row(const P2Row* p) {
+  const longlong2 r = stream_ld(reinterpret_cast<const longlong2*>(p));
+  return P2Row{r.x, r.y};
+}
+
 // Each segment's sub-bucket counts, hist[sg][b] (every one of the 2^logB2
-// written, zeros too).
-__global__ void __launch_bounds__(P2T) k_p2_hist(const long long* __restrict__ key, SegArgs g,
+// written, zeros too).  AOS: the side's rows are records.
+template <bool AOS>
+__global__ void __launch_bounds__(P2T) k_p2_hist(const long long* __restrict__ key,
+                                                 const P2Row* __restrict__ rec, SegArgs g,
                                                  int* __restrict__ hist) {
   __shared__ int bins[P2BINS];
   const int nb2 = 1 << g.logB2;
@@ -896,7 +923,7 @@ __global__ void __launch_bounds__(P2T) k_p2_hist(const long long* __restrict__ k
 #pragma unroll
       for (int q = 0; q < P2I; ++q) {
         const long long i = t0 + q * P2T + tid;
-        kk[q] = i < hi ? stream_ld(key + i) : 0;
+        kk[q] = i < hi ? (AOS ? stream_ld(&rec[i].k) : stream_ld(key + i)) : 0;
       }
 #pragma unroll
       for (int q = 0; q < P2I; ++q)
@@ -921,116 +948,159 @@ __global__ void k_p2_colsum(const int* __restrict__ hist, const int* __restrict_
   tot[idx] = run;
 }
 
-// A staged row: key and value in one 16-byte record (one shared-memory store
-// to place it, one load to write it out).
-struct alignas(16) P2Row {
-  long long k;
-  long long v;
-};
+// Region starts: cursor[i] = first[i] = i * cap for i < n.
+__global__ void k_region_starts(unsigned long long* __restrict__ cursor,
+                                unsigned long long* __restrict__ first, long long n,
+                                long long cap) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const unsigned long long s = (unsigned long long)(i * cap);
+    cursor[i] = s;
+    if (first) first[i] = s;
+  }
+}
 
-template <typename V>
+template <int BINS>
 struct P2Smem {
   P2Row sr[P2TILE];
-  int cnt[P2BINS];         // rows of a sub-bucket in the tile, then zero again
-  int lofs[P2BINS];        // a sub-bucket's first place in the tile
-  long long gpos[P2BINS];  // the sub-bucket's claimed first place in the output
+  int cnt[BINS];           // rows of a bin in the tile, then zero again
+  int lofs[BINS];          // a bin's first place in the tile
+  long long gpos[BINS];    // the bin's claimed first place in the output, -1: skip
   int wsum[P2T / 32];
 };
 
-// Rows to their sub-bucket's run, tile by tile in row order across the grid
-// (so the blocks at work at one time all append to the same run ends, and
-// each output line fills while it is in L2): each row's rank in its
-// sub-bucket (a shared-memory atomic), the tile's exclusive scan over the
-// sub-buckets, one claim per sub-bucket on its global cursor (travelling
-// while the tile is staged in shared memory in sub-bucket order), then the
-// write-out with consecutive threads on consecutive places (runs of about
+struct P2Args {
+  const long long* key;     // MODE 1/2: raw keys; MODE 0 build: hashes
+  const void* val;          // MODE 1 / MODE 0 build: int groups; MODE 2: int64 prices
+  const long long* disc;    // MODE 2: discounts, or null (the value is the price)
+  const P2Row* rec;         // MODE 0 probe: records
+  long long n;              // MODE 1/2: rows
+  long long scale;          // MODE 2: value = price * (scale - disc)
+  const long long* pstart;  // MODE 0: each partition's first row
+  const long long* pcnt;    // MODE 0: and rows
+  const int* tstart;        // MODE 0: [B + 1] each partition's first tile
+  int B;                    // MODE 0: partitions
+  int logS, logB2;          // bins: the 2^logB2 hash bits below the top logS - logB2
+  unsigned long long* cursor;  // per (sub-)bucket: its next free place
+  long long cap;            // > 0: bin id's region ends at (id + 1) * cap
+  unsigned long long* ovf;  // raised when a claim would cross its region's end
+  long long* key_out;       // SoA outputs (build side)
+  int* val_out;
+  P2Row* rec_out;           // AoS output (probe side)
+};
+
+// Rows to their bin's run, tile by tile (so the blocks at work at one time
+// all append to the same run ends, and each output line fills while it is in
+// L2): each row's rank in its bin (a shared-memory atomic), the tile's
+// exclusive scan over the bins, one claim per bin on its global cursor
+// (travelling while the tile is staged in shared memory in bin order), then
+// the write-out with consecutive threads on consecutive places (runs of about
 // P2TILE / 2^logB2 rows).  The next tile's rows are loaded before the
-// write-out.  A tile's sub-buckets are those of its first row's partition; a
-// row of the next partition (tiles that straddle a boundary) claims a place
-// of its own.  Order inside a sub-bucket is not kept.
+// write-out.  Order inside a bin is not kept.
 //
-// MODE 0 (the second pass): rows carry their hash and value.  The same kernel
-// is the shared-memory path's first pass with logS = logB2 = log2(B) (one
-// partition: the whole side, its buckets the sub-buckets): MODE 1 reads build
-// rows (key, group) and carries (mix64(key), group); MODE 2 reads probe rows
-// (fk, price, disc) and carries (mix64(fk), price * (scale - disc)), or
-// price when disc is null.
-// RI rows a thread a tile (a tile of P2T * RI <= P2TILE rows).
-template <typename V, int MODE, int RI = P2I>
-__global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(const long long* __restrict__ key_in,
-                                                       const V* __restrict__ val_in,
-                                                       const long long* __restrict__ disc_in,
-                                                       long long scale, long long n,
-                                                       int logS, int logB2,
-                                                       unsigned long long* __restrict__ cursor,
-                                                       long long* __restrict__ key_out,
-                                                       V* __restrict__ val_out) {
-  extern __shared__ __align__(16) unsigned char p2_smem[];
-  P2Smem<V>& S = *reinterpret_cast<P2Smem<V>*>(p2_smem);
-  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const int nb2 = 1 << logB2;
-  static_assert(P2T * RI <= P2TILE, "a tile fits the staging");
+// MODE 1 (first pass, build): rows (key, group) in row order, carried as
+// (mix64(key), group), bins = the B buckets.  MODE 2 (first pass, probe): rows
+// (fk, price, disc) carried as records (mix64(fk), price * (scale - disc)), or
+// price when disc is null.  MODE 0 (second pass): tiles run partition by
+// partition (tstart), the bins are the partition's 2^logB2 sub-buckets; the
+// build side reads and writes (hash, group) columns, the probe side records.
+// RI rows a thread a tile.
+template <int MODE, bool AOS, int BINS, int RI = P2I>
+__global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
+  using V = typename std::conditional<AOS, long long, int>::type;
+  constexpr int BPT = BINS / P2T;
   constexpr int TILE = P2T * RI;
-  const long long ntiles = (n + TILE - 1) / TILE;
-  const int bt = P2BPT * tid;  // the first of the sub-buckets this thread scans
+  constexpr int LOGBINS = BINS == 4096 ? 12 : BINS == 2048 ? 11 : 10;
+  static_assert(BINS == (1 << LOGBINS) && TILE <= P2TILE, "bins and tile");
+  extern __shared__ __align__(16) unsigned char p2_smem[];
+  P2Smem<BINS>& S = *reinterpret_cast<P2Smem<BINS>*>(p2_smem);
+  int* tps = reinterpret_cast<int*>(p2_smem + sizeof(P2Smem<BINS>));  // MODE 0
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int nb2 = 1 << a.logB2;
+  const int bt = BPT * tid;  // the first of the bins this thread scans
 #pragma unroll
-  for (int j = 0; j < P2BPT; ++j) S.cnt[bt + j] = 0;
+  for (int j = 0; j < BPT; ++j) S.cnt[bt + j] = 0;
+  long long ntiles;
+  if (MODE == 0) {
+    for (int p = tid; p <= a.B; p += P2T) tps[p] = a.tstart[p];
+    __syncthreads();
+    ntiles = tps[a.B];
+  } else {
+    ntiles = (a.n + TILE - 1) / TILE;
+  }
+  // tile t's rows [lo, hi) and its first bin's id
+  auto locate = [&](long long t, long long& lo, long long& hi, long long& base) {
+    if (MODE == 0) {
+      int l = 0, r = a.B;  // tps[l] <= t < tps[r]: the last partition starting at or before t
+      while (r - l > 1) {
+        const int m = (l + r) >> 1;
+        if (tps[m] <= t) l = m;
+        else r = m;
+      }
+      const long long p0 = a.pstart[l];
+      lo = p0 + (t - tps[l]) * TILE;
+      hi = min(lo + TILE, p0 + a.pcnt[l]);
+      base = (long long)l << a.logB2;
+    } else {
+      lo = t * TILE;
+      hi = min(lo + TILE, a.n);
+      base = 0;
+    }
+  };
   long long k[RI];
   V v[RI];
-  long long tile = blockIdx.x;
   // MODE 2 with a discount: the raw price in v and the discount in dv until
   // the tile's turn comes, so the prefetch never waits for its loads
   long long dv[MODE == 2 ? RI : 1];
-  long long k0 = 0;  // MODE 0: the tile's first key (its partition), loaded with the tile
-  auto load = [&](long long t) {
-    if (MODE == 0) k0 = key_in[t * TILE];
+  auto load = [&](long long lo, long long hi) {
 #pragma unroll
     for (int q = 0; q < RI; ++q) {
-      const long long i = t * TILE + q * P2T + tid;
-      if (i < n) {
-        k[q] = stream_ld(key_in + i);
-        v[q] = stream_ld(val_in + i);
-        if (MODE == 2 && disc_in) dv[q] = stream_ld(disc_in + i);
+      const long long i = lo + q * P2T + tid;
+      if (i < hi) {
+        if (MODE == 0 && AOS) {
+          const P2Row r = stream_ld_row(a.rec + i);
+          k[q] = r.k;
+          v[q] = (V)r.v;
+        } else {
+          k[q] = stream_ld(a.key + i);
+          v[q] = stream_ld(reinterpret_cast<const V*>(a.val) + i);
+        }
+        if (MODE == 2) dv[q] = a.disc ? stream_ld(a.disc + i) : 0;
       }
     }
   };
-  if (tile < ntiles) load(tile);
+  long long tile = blockIdx.x;
+  long long lo = 0, hi = 0, base = 0;
+  if (tile < ntiles) {
+    locate(tile, lo, hi, base);
+    load(lo, hi);
+  }
   __syncthreads();
   for (; tile < ntiles; tile += gridDim.x) {
-    const long long t0 = tile * TILE;
     if (MODE != 0) {
 #pragma unroll
       for (int q = 0; q < RI; ++q) k[q] = (long long)mix64((uint64_t)k[q]);
     }
-    if (MODE == 2 && disc_in) {
+    if (MODE == 2 && a.disc) {
 #pragma unroll
       for (int q = 0; q < RI; ++q)
-        v[q] = (V)(long long)((unsigned long long)v[q] * (unsigned long long)(scale - dv[q]));
+        v[q] = (V)(long long)((unsigned long long)v[q] * (unsigned long long)(a.scale - dv[q]));
     }
-    const long long base =
-        MODE != 0 ? 0 : ((long long)bucket_of_hash((uint64_t)k0, logS) >> logB2) << logB2;
-    int slot[RI];  // rank << P2MAXLOG | sub-bucket, or -1
+    int slot[RI];  // rank << LOGBINS | bin, or -1
 #pragma unroll
     for (int q = 0; q < RI; ++q) {
-      const long long i = t0 + q * P2T + tid;
       slot[q] = -1;
-      if (i < n) {
-        const long long id = bucket_of_hash((uint64_t)k[q], logS);
-        const unsigned long long b = (unsigned long long)(id - base);
-        if (b < (unsigned long long)nb2) {
-          slot[q] = (atomicAdd(&S.cnt[b], 1) << P2MAXLOG) | (int)b;
-        } else {
-          const long long pos = (long long)atomicAdd(&cursor[id], 1ULL);
-          key_out[pos] = k[q];
-          val_out[pos] = v[q];
-        }
+      if (lo + q * P2T + tid < hi) {
+        const int b = MODE == 0 ? (a.logB2 ? (int)(((uint64_t)k[q] >> (64 - a.logS)) & (nb2 - 1)) : 0)
+                                : bucket_of_hash((uint64_t)k[q], a.logS);
+        slot[q] = (atomicAdd(&S.cnt[b], 1) << LOGBINS) | b;
       }
     }
     __syncthreads();
-    int cb[P2BPT];
+    int cb[BPT];
     int s2 = 0;
 #pragma unroll
-    for (int j = 0; j < P2BPT; ++j) {
+    for (int j = 0; j < BPT; ++j) {
       cb[j] = S.cnt[bt + j];
       s2 += cb[j];
     }
@@ -1041,7 +1111,7 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(const long long*
     }
     if (lane == 31) S.wsum[w] = incl;
 #pragma unroll
-    for (int j = 0; j < P2BPT; ++j) S.cnt[bt + j] = 0;
+    for (int j = 0; j < BPT; ++j) S.cnt[bt + j] = 0;
     __syncthreads();
     int pre = 0, total = 0;
 #pragma unroll
@@ -1053,33 +1123,50 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(const long long*
     {
       int run = pre + incl - s2;
 #pragma unroll
-      for (int j = 0; j < P2BPT; ++j) {
+      for (int j = 0; j < BPT; ++j) {
         S.lofs[bt + j] = run;
         run += cb[j];
       }
     }
     __syncthreads();
     // the claims travel while the tile is placed
-    long long gp[P2BPT];
+    long long gp[BPT];
 #pragma unroll
-    for (int j = 0; j < P2BPT; ++j)
-      gp[j] = cb[j] ? (long long)atomicAdd(&cursor[base + bt + j], (unsigned long long)cb[j]) : 0;
+    for (int j = 0; j < BPT; ++j)
+      gp[j] = cb[j] ? (long long)atomicAdd(&a.cursor[base + bt + j], (unsigned long long)cb[j]) : 0;
 #pragma unroll
     for (int q = 0; q < RI; ++q) {
       if (slot[q] < 0) continue;
-      const int e = S.lofs[slot[q] & (P2BINS - 1)] + (slot[q] >> P2MAXLOG);
+      const int e = S.lofs[slot[q] & (BINS - 1)] + (slot[q] >> LOGBINS);
       S.sr[e] = P2Row{k[q], (long long)v[q]};
     }
 #pragma unroll
-    for (int j = 0; j < P2BPT; ++j) S.gpos[bt + j] = gp[j];
+    for (int j = 0; j < BPT; ++j) {
+      long long g = gp[j];
+      if (a.cap > 0 && cb[j] && g + cb[j] > (base + bt + j + 1) * a.cap) {
+        *a.ovf = 1;  // past the region: none of the bin's rows are written
+        g = -1;
+      }
+      S.gpos[bt + j] = g;
+    }
     __syncthreads();
-    if (tile + gridDim.x < ntiles) load(tile + gridDim.x);
+    if (tile + gridDim.x < ntiles) {
+      locate(tile + gridDim.x, lo, hi, base);
+      load(lo, hi);
+    }
     for (int e = tid; e < total; e += P2T) {
       const P2Row r = S.sr[e];
-      const int b = (int)(bucket_of_hash((uint64_t)r.k, logS) - base);
-      const long long pos = S.gpos[b] + (e - S.lofs[b]);
-      key_out[pos] = r.k;
-      val_out[pos] = (V)r.v;
+      const int b = MODE == 0 ? (a.logB2 ? (int)(((uint64_t)r.k >> (64 - a.logS)) & (nb2 - 1)) : 0)
+                              : bucket_of_hash((uint64_t)r.k, a.logS);
+      const long long g = S.gpos[b];
+      if (g < 0) continue;
+      const long long pos = g + (e - S.lofs[b]);
+      if (AOS) {
+        a.rec_out[pos] = r;
+      } else {
+        a.key_out[pos] = r.k;
+        a.val_out[pos] = (int)r.v;
+      }
     }
     __syncthreads();
   }
@@ -1088,16 +1175,18 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(const long long*
 struct SJArgs {
   const long long* bkey;
   const int* bgrp;
-  const long long* pfk;
-  const long long* pval;
-  const unsigned long long* bstart;  // [S + 1]
-  const unsigned long long* pstart;  // [S + 1]
+  const P2Row* prec;
+  const unsigned long long* bbeg;  // [S]: each sub-partition's build rows [bbeg, bend)
+  const unsigned long long* bend;
+  const unsigned long long* pbeg;  // and probe rows [pbeg, pend)
+  const unsigned long long* pend;
   long long S;
   int logS;
   long long group_min, n_groups;
   unsigned long long* slab;
   unsigned long long* stats;
   unsigned long long* counter;
+  const unsigned long long* ovf;   // nonzero: a region overflowed, nothing to join
 };
 
 // A cell's 64-bit sum in shared memory: with PF_SJ_SUM32, as two 32-bit
@@ -1143,7 +1232,6 @@ __device__ __forceinline__ void sj_sum_clear(SJSum& c) {
 struct SJSmem {
   long long key[SJ_TS];
   SJSum sum[SJ_TS];
-  unsigned goff[PF_SJ_NOGOFF ? 1 : SJ_TS];
   unsigned cnt[SJ_TS];
   unsigned short slot_of[SJ_CAP];  // the slot of each build row of the chunk
   long long min_sum;               // the key hashing to INT64_MIN, kept apart
@@ -1195,6 +1283,7 @@ __device__ __forceinline__ void sj_probe(SJSmem& S, long long key, long long val
 __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
   extern __shared__ __align__(16) unsigned char sj_smem[];
   SJSmem& S = *reinterpret_cast<SJSmem*>(sj_smem);
+  if (*a.ovf) return;  // the partitions are incomplete: the host runs the counted passes
   const int tid = threadIdx.x;
   for (int t = tid; t < SJ_TS; t += SJT) {
     S.key[t] = SJ_EMPTY;
@@ -1210,10 +1299,10 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
     const long long n = (long long)atomicAdd(a.counter, 1ULL);
     S.item[slot] = n;
     if (n < a.S) {
-      S.bnd[slot][0] = (long long)a.bstart[n];
-      S.bnd[slot][1] = (long long)a.bstart[n + 1];
-      S.bnd[slot][2] = (long long)a.pstart[n];
-      S.bnd[slot][3] = (long long)a.pstart[n + 1];
+      S.bnd[slot][0] = (long long)a.bbeg[n];
+      S.bnd[slot][1] = (long long)a.bend[n];
+      S.bnd[slot][2] = (long long)a.pbeg[n];
+      S.bnd[slot][3] = (long long)a.pend[n];
     }
   };
   if (tid == 0) {
@@ -1229,49 +1318,38 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
     const long long p0 = S.bnd[cur][2], p1 = S.bnd[cur][3];
     if (s >= a.S) break;
     if (tid == 0) fetch(cur ^ 1);
-    if (b1 == b0 || p1 == p0) {
+    if (b1 <= b0 || p1 <= p0) {
       __syncthreads();
       continue;
     }
     for (long long c0 = b0; c0 < b1; c0 += SJ_CAP) {
       const int nb = (int)min((long long)SJ_CAP, b1 - c0);
 #if PF_SJ_PIPE
-      // the first probe round's rows load while the build runs; pk / pv walk
+      // the first probe round's rows load while the build runs; pr walks
       // this thread's rows (every SJT-th from p0 + tid), rem counts the rows
       // from the current one to the end of the range
-      const long long* pk = a.pfk + p0 + tid;
-      const long long* pv = a.pval + p0 + tid;
+      const P2Row* pr = a.prec + p0 + tid;
       const long long rem = p1 - p0 - tid;
-      long long key[SJ_U], val[SJ_U];
+      P2Row row[SJ_U];
 #pragma unroll
-      for (int u = 0; u < SJ_U; ++u) {
-        key[u] = u * SJT < rem ? stream_ld(pk + u * SJT) : 0;
-        val[u] = u * SJT < rem ? stream_ld(pv + u * SJT) : 0;
-      }
+      for (int u = 0; u < SJ_U; ++u) row[u] = u * SJT < rem ? stream_ld_row(pr + u * SJT) : P2Row{0, 0};
 #endif
       // build: each build row a slot of its own (all of a thread's rows
       // loaded first)
       long long bk[SJ_BU];
-      int bg[SJ_BU];
 #pragma unroll
       for (int u = 0; u < SJ_BU; ++u) {
         const int j = u * SJT + tid;
-        if (j < nb) {
-          bk[u] = stream_ld(a.bkey + c0 + j);
-          bg[u] = stream_ld(a.bgrp + c0 + j);
-        }
+        if (j < nb) bk[u] = stream_ld(a.bkey + c0 + j);
       }
 #pragma unroll
       for (int u = 0; u < SJ_BU; ++u) {
         if (u * SJT + tid >= nb) continue;
         const long long key = bk[u];
-        const long long g = (long long)bg[u] - a.group_min;
-        unsigned goff = SJ_NONE;
-        if (g >= 0 && g < a.n_groups) goff = (unsigned)g;
-        else ++bad_group;
         if (key == SJ_EMPTY) {
+          const long long g = (long long)a.bgrp[c0 + u * SJT + tid] - a.group_min;
           S.has_min = 1;
-          S.min_goff = goff;
+          S.min_goff = g >= 0 && g < a.n_groups ? (unsigned)g : SJ_NONE;
           S.slot_of[u * SJT + tid] = 0xffff;
           continue;
         }
@@ -1280,10 +1358,7 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
           const long long old = (long long)atomicCAS((unsigned long long*)&S.key[t],
                                                      (unsigned long long)SJ_EMPTY,
                                                      (unsigned long long)key);
-          if (old == SJ_EMPTY) {
-            if (!PF_SJ_NOGOFF) S.goff[PF_SJ_NOGOFF ? 0 : t] = goff;
-            break;
-          }
+          if (old == SJ_EMPTY) break;
           t = sj_next(t);
         }
         S.slot_of[u * SJT + tid] = (unsigned short)t;
@@ -1293,73 +1368,222 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
 #if PF_SJ_PIPE
       // the next round's rows load while this round's are looked up
       {
-        long long nkey[SJ_U], nval[SJ_U];
+        P2Row nrow[SJ_U];
         constexpr int STEP = SJT * SJ_U;
         for (long long r = rem; r > 0; r -= STEP) {
-          pk += STEP;
-          pv += STEP;
+          pr += STEP;
           const long long rn = r - STEP;
 #pragma unroll
-          for (int u = 0; u < SJ_U; ++u) {
-            nkey[u] = u * SJT < rn ? stream_ld(pk + u * SJT) : 0;
-            nval[u] = u * SJT < rn ? stream_ld(pv + u * SJT) : 0;
-          }
+          for (int u = 0; u < SJ_U; ++u)
+            nrow[u] = u * SJT < rn ? stream_ld_row(pr + u * SJT) : P2Row{0, 0};
 #pragma unroll
           for (int u = 0; u < SJ_U; ++u)
-            if (u * SJT < r) sj_probe(S, key[u], val[u], a.logS, matched);
+            if (u * SJT < r) sj_probe(S, row[u].k, row[u].v, a.logS, matched);
 #pragma unroll
-          for (int u = 0; u < SJ_U; ++u) {
-            key[u] = nkey[u];
-            val[u] = nval[u];
-          }
+          for (int u = 0; u < SJ_U; ++u) row[u] = nrow[u];
         }
       }
 #else
       for (long long i0 = p0; i0 < p1; i0 += (long long)SJT * SJ_U) {
-        long long key[SJ_U], val[SJ_U];
+        P2Row row[SJ_U];
 #pragma unroll
         for (int u = 0; u < SJ_U; ++u) {
           const long long i = i0 + u * SJT + tid;
-          if (i < p1) {
-            key[u] = stream_ld(a.pfk + i);
-            val[u] = stream_ld(a.pval + i);
-          }
+          if (i < p1) row[u] = stream_ld_row(a.prec + i);
         }
 #pragma unroll
         for (int u = 0; u < SJ_U; ++u)
-          if (i0 + u * SJT + tid < p1) sj_probe(S, key[u], val[u], a.logS, matched);
+          if (i0 + u * SJT + tid < p1) sj_probe(S, row[u].k, row[u].v, a.logS, matched);
       }
 #endif
       __syncthreads();
-      // flush every build row that matched, and empty its slot
+      // flush every build row that matched (its group read again, from L2),
+      // and empty its slot
       for (int j = tid; j < nb; j += SJT) {
         const unsigned t = S.slot_of[j];
         if (t == 0xffff) continue;
         const unsigned c = S.cnt[t];
-        unsigned go;
-        if (PF_SJ_NOGOFF) {
-          const long long g = (long long)a.bgrp[c0 + j] - a.group_min;
-          go = g >= 0 && g < a.n_groups ? (unsigned)g : SJ_NONE;
-        } else {
-          go = S.goff[t];
-        }
-        if (c && go != SJ_NONE) {
-          atomicAdd(&a.slab[2 * (unsigned long long)go], sj_sum_get(S.sum[t]));
-          atomicAdd(&a.slab[2 * (unsigned long long)go + 1], (unsigned long long)c);
+        const long long g = (long long)a.bgrp[c0 + j] - a.group_min;
+        const bool gok = g >= 0 && g < a.n_groups;
+        bad_group += !gok;
+        if (c && gok) {
+          atomicAdd(&a.slab[2 * (unsigned long long)g], sj_sum_get(S.sum[t]));
+          atomicAdd(&a.slab[2 * (unsigned long long)g + 1], (unsigned long long)c);
         }
         S.key[t] = SJ_EMPTY;
         sj_sum_clear(S.sum[t]);
         S.cnt[t] = 0;
       }
       if (tid == 0) {
-        if (S.has_min && S.min_cnt && S.min_goff != SJ_NONE) {
-          atomicAdd(&a.slab[2 * (unsigned long long)S.min_goff], (unsigned long long)S.min_sum);
-          atomicAdd(&a.slab[2 * (unsigned long long)S.min_goff + 1],
-                    (unsigned long long)S.min_cnt);
+        if (S.has_min) {
+          bad_group += S.min_goff == SJ_NONE;
+          if (S.min_cnt && S.min_goff != SJ_NONE) {
+            atomicAdd(&a.slab[2 * (unsigned long long)S.min_goff], (unsigned long long)S.min_sum);
+            atomicAdd(&a.slab[2 * (unsigned long long)S.min_goff + 1],
+                      (unsigned long long)S.min_cnt);
+          }
         }
         S.has_min = 0;
         S.min_sum = 0;
         S.min_cnt = 0;
+      }
+      __syncthreads();
+    }
+  }
+  unsigned long long m = matched;
+  for (int o = 16; o; o >>= 1) m += __shfl_xor_sync(FULL, m, o);
+  if ((tid & 31) == 0 && m) atomicAdd(&a.stats[0], m);
+  if (bad_group) atomicAdd(&a.stats[2], bad_group);
+}
+
+// ---- the join with a fingerprinted slot table ----------------------------------
+//
+// The same join per sub-partition with the table split in three: 4-byte
+// slots {build row + 1 (11 bits) | fingerprint (21 low hash bits)}, 0 = free,
+// at a load of at most 0.375; the chunk's build hashes by row; and the cells
+// (sum as two 32-bit words, count) by row.  A probe row walks slots until a
+// free one, reading a build row's hash only where the fingerprint agrees.
+// 4-byte slots let the table be larger for the same shared memory (shorter
+// walks, fewer divergent lanes), the cells are flushed in row order, and no
+// hash value is reserved as a free mark.
+#ifndef PF_SJF_LOGTS
+#define PF_SJF_LOGTS 12
+#endif
+#ifndef PF_SJF_T
+#define PF_SJF_T 384
+#endif
+#ifndef PF_SJF_MINB
+#define PF_SJF_MINB 4
+#endif
+constexpr int SJF_TS = 1 << PF_SJF_LOGTS;   // slots
+constexpr int SJF_T = PF_SJF_T;              // threads
+constexpr int SJF_CAP = 1536;                // build rows a chunk (row + 1 fits 11 bits)
+constexpr int SJF_BU = (SJF_CAP + SJF_T - 1) / SJF_T;
+constexpr unsigned SJF_FPBITS = 21;
+constexpr unsigned SJF_FPMASK = (1u << SJF_FPBITS) - 1;
+static_assert(SJF_CAP < (1 << (32 - SJF_FPBITS)), "row + 1 fits the slot's high bits");
+static_assert(SJF_CAP * 8 <= SJF_TS * 3, "load at most 0.375");
+
+struct SJFSmem {
+  unsigned slot[SJF_TS];
+  long long bh[SJF_CAP];           // the chunk's build hashes by row
+  unsigned lo[SJF_CAP], hi[SJF_CAP], cnt[SJF_CAP];
+  unsigned short slot_of[SJF_CAP]; // each build row's slot (to free it)
+  long long item[2];               // sub-partition and its row ranges, double-buffered
+  long long bnd[2][4];
+};
+
+__device__ __forceinline__ unsigned sjf_home(uint64_t h, int logS) {
+  if (logS + PF_SJF_LOGTS <= 32) return ((unsigned)(h >> 32) << logS) >> (32 - PF_SJF_LOGTS);
+  return (unsigned)((h << logS) >> (64 - PF_SJF_LOGTS));
+}
+
+__global__ void __launch_bounds__(SJF_T, PF_SJF_MINB) k_sjoin_fp(SJArgs a) {
+  extern __shared__ __align__(16) unsigned char sjf_smem[];
+  SJFSmem& S = *reinterpret_cast<SJFSmem*>(sjf_smem);
+  if (*a.ovf) return;  // the partitions are incomplete: the host runs the counted passes
+  const int tid = threadIdx.x;
+  for (int t = tid; t < SJF_TS; t += SJF_T) S.slot[t] = 0;
+  for (int r = tid; r < SJF_CAP; r += SJF_T) {
+    S.lo[r] = 0;
+    S.hi[r] = 0;
+    S.cnt[r] = 0;
+  }
+  unsigned matched = 0;
+  unsigned long long bad_group = 0;
+  auto fetch = [&](int slot) {
+    const long long n = (long long)atomicAdd(a.counter, 1ULL);
+    S.item[slot] = n;
+    if (n < a.S) {
+      S.bnd[slot][0] = (long long)a.bbeg[n];
+      S.bnd[slot][1] = (long long)a.bend[n];
+      S.bnd[slot][2] = (long long)a.pbeg[n];
+      S.bnd[slot][3] = (long long)a.pend[n];
+    }
+  };
+  if (tid == 0) fetch(0);
+  __syncthreads();
+  for (int cur = 0;; cur ^= 1) {
+    const long long s = S.item[cur];
+    const long long b0 = S.bnd[cur][0], b1 = S.bnd[cur][1];
+    const long long p0 = S.bnd[cur][2], p1 = S.bnd[cur][3];
+    if (s >= a.S) break;
+    if (tid == 0) fetch(cur ^ 1);
+    if (b1 <= b0 || p1 <= p0) {
+      __syncthreads();
+      continue;
+    }
+    for (long long c0 = b0; c0 < b1; c0 += SJF_CAP) {
+      const int nb = (int)min((long long)SJF_CAP, b1 - c0);
+      // the first probe round's rows load while the build runs
+      const P2Row* pr = a.prec + p0 + tid;
+      const long long rem = p1 - p0 - tid;
+      P2Row row = rem > 0 ? stream_ld_row(pr) : P2Row{0, 0};
+      long long bk[SJF_BU];
+#pragma unroll
+      for (int u = 0; u < SJF_BU; ++u) {
+        const int j = u * SJF_T + tid;
+        if (j < nb) bk[u] = stream_ld(a.bkey + c0 + j);
+      }
+#pragma unroll
+      for (int u = 0; u < SJF_BU; ++u) {
+        const int j = u * SJF_T + tid;
+        if (j >= nb) continue;
+        const uint64_t h = (uint64_t)bk[u];
+        S.bh[j] = (long long)h;
+        const unsigned e = ((unsigned)(j + 1) << SJF_FPBITS) | ((unsigned)h & SJF_FPMASK);
+        unsigned t = sjf_home(h, a.logS);
+        for (int probes = 0; probes < SJF_TS; ++probes) {
+          if (atomicCAS(&S.slot[t], 0u, e) == 0u) break;
+          t = (t + 1) & (SJF_TS - 1);
+        }
+        S.slot_of[j] = (unsigned short)t;
+      }
+      __syncthreads();
+      // probe: the next round's row loads while this one's is looked up
+      for (long long r = rem; r > 0; r -= SJF_T) {
+        pr += SJF_T;
+        const P2Row next = r > SJF_T ? stream_ld_row(pr) : P2Row{0, 0};
+        const uint64_t h = (uint64_t)row.k;
+        const unsigned fp = (unsigned)h & SJF_FPMASK;
+        unsigned t = sjf_home(h, a.logS);
+        for (int probes = 0; probes < SJF_TS; ++probes) {
+          const unsigned e = S.slot[t];
+          if (e == 0u) break;
+          if ((e & SJF_FPMASK) == fp) {
+            const int j = (int)(e >> SJF_FPBITS) - 1;
+            if ((uint64_t)S.bh[j] == h) {
+              const unsigned l = (unsigned)(unsigned long long)row.v;
+              const unsigned hw = (unsigned)((unsigned long long)row.v >> 32);
+              const unsigned old = atomicAdd(&S.lo[j], l);
+              const unsigned hc = hw + (old + l < old ? 1u : 0u);
+              if (hc) atomicAdd(&S.hi[j], hc);
+              atomicAdd(&S.cnt[j], 1u);
+              ++matched;
+              break;
+            }
+          }
+          t = (t + 1) & (SJF_TS - 1);
+        }
+        row = next;
+      }
+      __syncthreads();
+      // flush every build row that matched (its group read again, from L2),
+      // and free its slot and cell
+      for (int j = tid; j < nb; j += SJF_T) {
+        const unsigned c = S.cnt[j];
+        const long long g = (long long)a.bgrp[c0 + j] - a.group_min;
+        const bool gok = g >= 0 && g < a.n_groups;
+        bad_group += !gok;
+        if (c && gok) {
+          atomicAdd(&a.slab[2 * (unsigned long long)g],
+                    ((unsigned long long)S.hi[j] << 32) | S.lo[j]);
+          atomicAdd(&a.slab[2 * (unsigned long long)g + 1], (unsigned long long)c);
+        }
+        S.slot[S.slot_of[j]] = 0;
+        S.lo[j] = 0;
+        S.hi[j] = 0;
+        S.cnt[j] = 0;
       }
       __syncthreads();
     }
@@ -1480,15 +1704,19 @@ void chunking(long long n, long long* chunk, int* nchunks) {
   *nchunks = (int)std::max<long long>(1, (n + *chunk - 1) / *chunk);
 }
 
+// The passes the calling thread's last call counted first (bit 0: first, bit 1:
+// second).
+thread_local int g_counted_passes = 0;
+
 struct JaLayout {
   int* hist_b;
   int* hist_p;
   long long* cnt;      // [2B]: build counts, probe counts
   long long* start;    // [2B]: build starts, probe starts
   long long* total;    // [2]
-  long long* pkey;
+  long long* pkey;     // the first pass's build side (hash or key, group)
   int* pgrp;
-  long long* pfk;
+  long long* pfk;      // the round path's probe side (key, value)
   long long* pval;
   Slot* table;
   long long table_slots;
@@ -1497,22 +1725,34 @@ struct JaLayout {
   long long max_launches;
   unsigned* counters;        // [max_launches] work counters of the round launches
   // the shared-memory path
+  long long cap1[2];         // rows of a first-pass bucket's region, per side
+  P2Row* prec;               // the first pass's probe side (records)
   long long s_max;           // sub-partitions at most
+  long long rows2[2];        // rows of the second pass's output, per side
   long long* pkey2;
   int* pgrp2;
-  long long* pfk2;
-  long long* pval2;
-  long long nseg_max[2];       // pass-2 segments a side, at most
-  int2* seg2[2];               // the segments of each side
-  int* pseg2[2];               // [B + 1]: each partition's first segment
-  int* hist2[2];               // [segments][2^logB2]
-  unsigned long long* cur2;    // [2][s_max]: the pass-2 scatter's cursors
-  unsigned long long* cur1;    // [2B]: the tile scatter's cursors in the first pass
-  long long* tot2;             // [2][s_max]: rows per sub-partition
+  P2Row* prec2;
+  long long* pstart;         // [2B]: each side's partition starts, then [2B] rows
+  int* tstart[2];            // [B + 1]: each partition's first second-pass tile
+  long long nseg_max[2];     // counted second pass: segments a side, at most
+  int2* seg2[2];             // the segments of each side
+  int* pseg2[2];             // [B + 1]: each partition's first segment
+  int* hist2[2];             // [segments][2^logB2]
+  unsigned long long* cur2;    // [2][s_max]: the second pass's cursors
+  unsigned long long* beg2;    // [2][s_max]: its regions' starts
+  unsigned long long* cur1;    // [2B]: the first pass's cursors
+  long long* tot2;             // [2][s_max]: rows per sub-partition (counted)
   unsigned long long* start2;  // [2][s_max + 1]
   long long* scan2;            // scan scratch
   unsigned long long* sj_counter;
+  unsigned long long* ovf;     // [2]: a region of the first / second pass overflowed
 };
+
+// Sub-partitions a partition splits into at most (a power of two), and the
+// table of the shared-memory path: never finer than SJ_TARGET build rows.
+long long max_subparts(long long nb) {
+  return std::min<long long>(P2BINS, (long long)pow2_at_least((uint64_t)(nb / SJ_TARGET + 1)));
+}
 
 JaLayout ja_layout(Arena& a, long long nb, long long np, int B, long long n_groups) {
   JaLayout l{};
@@ -1525,42 +1765,54 @@ JaLayout ja_layout(Arena& a, long long nb, long long np, int B, long long n_grou
   l.cnt = a.take<long long>(2 * (size_t)B);
   l.start = a.take<long long>(2 * (size_t)B);
   l.total = a.take<long long>(2);
-  l.pkey = a.take<long long>(std::max<long long>(nb, 1));
-  l.pgrp = a.take<int>(std::max<long long>(nb, 1));
-  l.pfk = a.take<long long>(std::max<long long>(np, 1));
-  l.pval = a.take<long long>(std::max<long long>(np, 1));
-  // two halves, one built while the other is probed
-  l.table_slots = 2 * std::max<long long>(1, std::min(nb, round_rows()));
-  l.table = a.take<Slot>(2 * l.table_slots);
   l.reg = a.take<long long>(2 * (size_t)B);
   l.slab = a.take<unsigned long long>(2 * (size_t)std::max<long long>(n_groups, 1));
-  // one work counter per launch: at most B whole-partition rounds plus the
-  // slices of partitions over the budget, plus one
-  l.max_launches = B + nb / std::max<long long>(1, l.table_slots / 2) + 2;
-  l.counters = a.take<unsigned>(l.max_launches);
-  if (join_path_smem()) {
-    // a partition splits into at most 2^P2MAXLOG sub-partitions, and never
-    // finer than SJ_TARGET build rows
-    l.s_max = (long long)B * std::min<long long>(
-                                 P2BINS, (long long)pow2_at_least((uint64_t)(nb / SJ_TARGET + 1)));
-    l.pkey2 = a.take<long long>(std::max<long long>(nb, 1));
-    l.pgrp2 = a.take<int>(std::max<long long>(nb, 1));
-    l.pfk2 = a.take<long long>(std::max<long long>(np, 1));
-    l.pval2 = a.take<long long>(std::max<long long>(np, 1));
-    const long long rows[2] = {nb, np};
-    for (int side = 0; side < 2; ++side) {
-      l.nseg_max[side] = rows[side] / P2SEG + B + 1;
-      l.seg2[side] = a.take<int2>((size_t)l.nseg_max[side]);
-      l.pseg2[side] = a.take<int>((size_t)B + 1);
-      l.hist2[side] = a.take<int>((size_t)l.nseg_max[side] * P2BINS);
-    }
-    l.tot2 = a.take<long long>(2 * (size_t)l.s_max);
-    l.cur2 = a.take<unsigned long long>(2 * (size_t)l.s_max);
-    l.cur1 = a.take<unsigned long long>(2 * (size_t)B);
-    l.start2 = a.take<unsigned long long>(2 * ((size_t)l.s_max + 1));
-    l.scan2 = a.take<long long>(scan_scratch_elems(l.s_max));
-    l.sj_counter = a.take<unsigned long long>(1);
+  l.ovf = a.take<unsigned long long>(2);
+  if (!join_path_smem()) {
+    l.pkey = a.take<long long>(std::max<long long>(nb, 1));
+    l.pgrp = a.take<int>(std::max<long long>(nb, 1));
+    l.pfk = a.take<long long>(std::max<long long>(np, 1));
+    l.pval = a.take<long long>(std::max<long long>(np, 1));
+    // two halves, one built while the other is probed
+    l.table_slots = 2 * std::max<long long>(1, std::min(nb, round_rows()));
+    l.table = a.take<Slot>(2 * l.table_slots);
+    // one work counter per launch: at most B whole-partition rounds plus the
+    // slices of partitions over the budget, plus one
+    l.max_launches = B + nb / std::max<long long>(1, l.table_slots / 2) + 2;
+    l.counters = a.take<unsigned>(l.max_launches);
+    return l;
   }
+  // first pass: a region of cap1 rows a bucket (at least the side's rows)
+  const long long rows[2] = {nb, np};
+  for (int side = 0; side < 2; ++side)
+    l.cap1[side] = std::max((rows[side] + B - 1) / B, region_rows((double)rows[side] / B));
+  l.pkey = a.take<long long>((size_t)B * l.cap1[0]);
+  l.pgrp = a.take<int>((size_t)B * l.cap1[0]);
+  l.prec = a.take<P2Row>((size_t)B * l.cap1[1]);
+  // second pass: regions for partitions as full as the first pass's regions
+  const long long b2 = max_subparts(nb);
+  l.s_max = (long long)B * b2;
+  for (int side = 0; side < 2; ++side)
+    l.rows2[side] = std::max(std::max<long long>(rows[side], 1),
+                             l.s_max * region_rows((double)l.cap1[side] / b2));
+  l.pkey2 = a.take<long long>((size_t)l.rows2[0]);
+  l.pgrp2 = a.take<int>((size_t)l.rows2[0]);
+  l.prec2 = a.take<P2Row>((size_t)l.rows2[1]);
+  l.pstart = a.take<long long>(4 * (size_t)B);
+  for (int side = 0; side < 2; ++side) {
+    l.tstart[side] = a.take<int>((size_t)B + 1);
+    l.nseg_max[side] = rows[side] / P2SEG + B + 1;
+    l.seg2[side] = a.take<int2>((size_t)l.nseg_max[side]);
+    l.pseg2[side] = a.take<int>((size_t)B + 1);
+    l.hist2[side] = a.take<int>((size_t)l.nseg_max[side] * P2BINS);
+  }
+  l.tot2 = a.take<long long>(2 * (size_t)l.s_max);
+  l.cur2 = a.take<unsigned long long>(2 * (size_t)l.s_max);
+  l.beg2 = a.take<unsigned long long>(2 * (size_t)l.s_max);
+  l.cur1 = a.take<unsigned long long>(2 * (size_t)B);
+  l.start2 = a.take<unsigned long long>(2 * ((size_t)l.s_max + 1));
+  l.scan2 = a.take<long long>(scan_scratch_elems(l.s_max));
+  l.sj_counter = a.take<unsigned long long>(1);
   return l;
 }
 
@@ -1589,113 +1841,177 @@ long long* pinned_counts(size_t n) {
 }
 
 
-// The first radix pass of both sides (the TMA-fed kernel when every column
-// is 16-byte aligned).
-template <bool HASHED>
-int fscatter_both(bool tma, const int64_t* build_key, const int32_t* build_group, long long n_build,
-                  const int64_t* probe_fk, const int64_t* probe_price, const int64_t* probe_disc,
-                  long long scale, long long n_probe, long long chunk_b, int nch_b,
-                  long long chunk_p, int nch_p, int logB, int B, const JaLayout& l,
-                  int64_t* stats_out, cudaStream_t st) {
+// The round path's first radix pass of both sides (the TMA-fed kernel when
+// every column is 16-byte aligned).
+int fscatter_rounds(bool tma, const int64_t* build_key, const int32_t* build_group,
+                    long long n_build, const int64_t* probe_fk, const int64_t* probe_price,
+                    const int64_t* probe_disc, long long scale, long long n_probe,
+                    long long chunk_b, int nch_b, long long chunk_p, int nch_p, int logB, int B,
+                    const JaLayout& l, int64_t* stats_out, cudaStream_t st) {
   if (tma) {
     const size_t smb = tma_smem<false>(B), smp = tma_smem<true>(B);
-    if (int rc = opt_in_smem((const void*)k_fscatter_tma<false, HASHED>, smb)) return rc;
-    if (int rc = opt_in_smem((const void*)k_fscatter_tma<true, HASHED>, smp)) return rc;
+    if (int rc = opt_in_smem((const void*)k_fscatter_tma<false, false>, smb)) return rc;
+    if (int rc = opt_in_smem((const void*)k_fscatter_tma<true, false>, smp)) return rc;
     {
       PF_KERNEL("k_fscatter_build", st);
-      k_fscatter_tma<false, HASHED><<<nch_b, TT, smb, st>>>(
+      k_fscatter_tma<false, false><<<nch_b, TT, smb, st>>>(
           (const long long*)build_key, build_group, nullptr, 0, n_build, chunk_b, logB, B,
           tma_nbuf<false>(B), l.hist_b, l.start, l.pkey, l.pgrp, (unsigned long long*)stats_out + 1);
     }
     {
       PF_KERNEL("k_fscatter_probe", st);
-      k_fscatter_tma<true, HASHED><<<nch_p, TT, smp, st>>>(
+      k_fscatter_tma<true, false><<<nch_p, TT, smp, st>>>(
           (const long long*)probe_fk, probe_price, (const long long*)probe_disc, scale, n_probe,
           chunk_p, logB, B, tma_nbuf<true>(B), l.hist_p, l.start + B, l.pfk, l.pval,
           (unsigned long long*)stats_out + 1);
     }
   } else {
     const size_t smb = fscatter_smem(B, false), smp = fscatter_smem(B, true);
-    if (int rc = opt_in_smem((const void*)k_fscatter<false, HASHED>, smb)) return rc;
-    if (int rc = opt_in_smem((const void*)k_fscatter<true, HASHED>, smp)) return rc;
+    if (int rc = opt_in_smem((const void*)k_fscatter<false, false>, smb)) return rc;
+    if (int rc = opt_in_smem((const void*)k_fscatter<true, false>, smp)) return rc;
     {
       PF_KERNEL("k_fscatter_build", st);
-      k_fscatter<false, HASHED><<<nch_b, FT, smb, st>>>((const long long*)build_key, build_group, nullptr, 0,
-                                                n_build, chunk_b, logB, B, l.hist_b, l.start, l.pkey,
-                                                l.pgrp);
+      k_fscatter<false, false><<<nch_b, FT, smb, st>>>((const long long*)build_key, build_group,
+                                                       nullptr, 0, n_build, chunk_b, logB, B,
+                                                       l.hist_b, l.start, l.pkey, l.pgrp);
     }
     {
       PF_KERNEL("k_fscatter_probe", st);
-      k_fscatter<true, HASHED><<<nch_p, FT, smp, st>>>((const long long*)probe_fk, probe_price,
-                                               (const long long*)probe_disc, scale, n_probe, chunk_p,
-                                               logB, B, l.hist_p, l.start + B, l.pfk, l.pval);
+      k_fscatter<true, false><<<nch_p, FT, smp, st>>>((const long long*)probe_fk, probe_price,
+                                                      (const long long*)probe_disc, scale, n_probe,
+                                                      chunk_p, logB, B, l.hist_p, l.start + B,
+                                                      l.pfk, l.pval);
     }
   }
   return ok();
 }
 
-// The shared-memory path's first pass through the tile scatter (B <= P2BINS):
-// cursors from the bucket starts, each side's rows hashed and carried with
-// their value.
-int first_pass_tile(const int64_t* build_key, const int32_t* build_group, long long n_build,
-                    const int64_t* probe_fk, const int64_t* probe_price, const int64_t* probe_disc,
-                    long long scale, long long n_probe, int logB, int B, const JaLayout& l,
-                    cudaStream_t st) {
-  PF_CUDA(cudaMemcpyAsync(l.cur1, l.start, 2 * (size_t)B * sizeof(long long),
-                          cudaMemcpyDeviceToDevice, st));
-  const size_t sb = sizeof(P2Smem<int>), sp = sizeof(P2Smem<long long>);
-  if (int rc = opt_in_smem((const void*)k_p2_scatter<int, 1>, sb)) return rc;
-  if (int rc = opt_in_smem((const void*)k_p2_scatter<long long, 2, P2RI2>, sp)) return rc;
-  int ob = 0, op = 0;
-  PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ob, k_p2_scatter<int, 1>, P2T, sb));
-  PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&op, k_p2_scatter<long long, 2, P2RI2>,
-                                                        P2T, sp));
-  const int sms = sm_count();
-  const unsigned gb = (unsigned)std::max<long long>(
-      1, std::min<long long>((n_build + P2TILE - 1) / P2TILE, (long long)std::max(1, ob) * sms));
-  constexpr int tile2 = P2T * P2RI2;
-  const unsigned gp = (unsigned)std::max<long long>(
-      1, std::min<long long>((n_probe + tile2 - 1) / tile2, (long long)std::max(1, op) * sms));
+// Both sides' bucket counts and starts (the counted first pass and the round
+// path): per-chunk histograms, per-bucket chunk offsets, the starts, and the
+// counts copied into `hc` (pinned) behind the returned event.
+int count_buckets(const int64_t* build_key, long long n_build, const int64_t* probe_fk,
+                  long long n_probe, int logB, int B, const JaLayout& l, long long* hc,
+                  cudaEvent_t* ev, cudaStream_t st) {
+  long long chunk_b, chunk_p;
+  int nch_b, nch_p;
+  chunking(n_build, &chunk_b, &nch_b);
+  chunking(n_probe, &chunk_p, &nch_p);
+  const size_t hsm = (size_t)B * sizeof(int);
+  if (int rc = opt_in_smem((const void*)k_fhist, hsm)) return rc;
   {
-    PF_KERNEL("k_fscatter_build", st);
-    k_p2_scatter<int, 1><<<gb, P2T, sb, st>>>((const long long*)build_key, build_group, nullptr, 0,
-                                              n_build, logB, logB, l.cur1, l.pkey, l.pgrp);
+    PF_KERNEL("k_fhist", st);
+    k_fhist<<<nch_b, FT, hsm, st>>>((const long long*)build_key, n_build, chunk_b, logB, B, l.hist_b);
   }
   {
-    PF_KERNEL("k_fscatter_probe", st);
-    k_p2_scatter<long long, 2, P2RI2><<<gp, P2T, sp, st>>>(
-        (const long long*)probe_fk, (const long long*)probe_price, (const long long*)probe_disc,
-        scale, n_probe, logB, logB, l.cur1 + B, l.pfk, l.pval);
+    PF_KERNEL("k_fhist", st);
+    k_fhist<<<nch_p, FT, hsm, st>>>((const long long*)probe_fk, n_probe, chunk_p, logB, B, l.hist_p);
   }
-  PF_LAUNCH("k_fscatter");
+  PF_LAUNCH("k_fhist");
+  {
+    PF_KERNEL("k_fscan", st);
+    k_fscan<<<(B + 31) / 32, FT, 0, st>>>(l.hist_b, nch_b, B, l.cnt);
+  }
+  {
+    PF_KERNEL("k_fscan", st);
+    k_fscan<<<(B + 31) / 32, FT, 0, st>>>(l.hist_p, nch_p, B, l.cnt + B);
+  }
+  PF_LAUNCH("k_fscan");
+  PF_CUDA(cudaMemcpyAsync(l.start, l.cnt, 2 * B * sizeof(long long), cudaMemcpyDeviceToDevice, st));
+  {
+    PF_KERNEL("k_scan_counts", st);
+    k_scan_counts<<<1, 1024, 0, st>>>(l.start, B, l.total, nullptr);
+  }
+  {
+    PF_KERNEL("k_scan_counts", st);
+    k_scan_counts<<<1, 1024, 0, st>>>(l.start + B, B, l.total + 1, nullptr);
+  }
+  PF_LAUNCH("k_scan_counts");
+  PF_CUDA(cudaMemcpyAsync(hc, l.cnt, 2 * B * sizeof(long long), cudaMemcpyDeviceToHost, st));
+  return record_event(st, ev);
+}
+
+// Launch shape of a tile scatter: opt in to its shared memory, then one
+// block a tile up to the resident blocks of every SM.
+template <int MODE, bool AOS, int BINS, int RI>
+int p2_launch(const P2Args& a, long long ntiles, size_t extra_smem, const char* name,
+              cudaStream_t st) {
+  if (ntiles <= 0) return ok();
+  const size_t sm = sizeof(P2Smem<BINS>) + extra_smem;
+  auto kern = k_p2_scatter<MODE, AOS, BINS, RI>;
+  if (int rc = opt_in_smem((const void*)kern, sm)) return rc;
+  int per_sm = 0;
+  PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, P2T, sm));
+  const unsigned g = (unsigned)std::max<long long>(
+      1, std::min<long long>(ntiles, (long long)std::max(1, per_sm) * sm_count()));
+  {
+    PF_KERNEL(name, st);
+    kern<<<g, P2T, sm, st>>>(a);
+  }
+  PF_LAUNCH(name);
   return ok();
 }
 
-// The shared-memory path after the first scatter (counts on the host): the
-// second radix pass into sub-partitions of about SJ_TARGET build rows, the
-// join per sub-partition, the slab split.  Keys are mix64 hashes here.
-int join_smem(const JaLayout& l, int B, int logB, const long long* hc, long long n_build,
-              long long n_probe, long long group_min, long long n_groups, int64_t* sum_out,
-              int64_t* count_out, int64_t* stats_out, cudaStream_t st) {
-  long long maxp = 0;
-  for (int p = 0; p < B; ++p) maxp = std::max(maxp, hc[p]);
-  int logB2 = 0;
-  while ((maxp >> logB2) > SJ_TARGET && logB2 < P2MAXLOG &&
-         ((long long)B << (logB2 + 1)) <= l.s_max)
-    ++logB2;
-  const int logS = logB + logB2;
-  const long long S = 1LL << logS;
+// The shared-memory path's first pass: both sides hashed and scattered by
+// the tile scatter into B buckets, from the cursors in l.cur1; cap > 0: into
+// regions of cap rows a bucket (an overflow raises ovf[0]).
+int first_pass(const int64_t* build_key, const int32_t* build_group, long long n_build,
+               const int64_t* probe_fk, const int64_t* probe_price, const int64_t* probe_disc,
+               long long scale, long long n_probe, int logB, int B, const long long cap[2],
+               const JaLayout& l, cudaStream_t st) {
+  P2Args b{};
+  b.key = (const long long*)build_key;
+  b.val = build_group;
+  b.n = n_build;
+  b.logS = b.logB2 = logB;
+  b.cursor = l.cur1;
+  b.cap = cap[0];
+  b.ovf = l.ovf;
+  b.key_out = l.pkey;
+  b.val_out = l.pgrp;
+  P2Args p{};
+  p.key = (const long long*)probe_fk;
+  p.val = probe_price;
+  p.disc = (const long long*)probe_disc;
+  p.scale = scale;
+  p.n = n_probe;
+  p.logS = p.logB2 = logB;
+  p.cursor = l.cur1 + B;
+  p.cap = cap[1];
+  p.ovf = l.ovf;
+  p.rec_out = l.prec;
+  constexpr int tb = P2TILE, tp = P2T * P2RI2;
+  if (B <= P2BINS) {
+    if (int rc = p2_launch<1, false, P2BINS, P2I>(b, (n_build + tb - 1) / tb, 0,
+                                                  "k_fscatter_build", st))
+      return rc;
+    return p2_launch<2, true, P2BINS, P2RI2>(p, (n_probe + tp - 1) / tp, 0, "k_fscatter_probe",
+                                             st);
+  }
+  if (int rc = p2_launch<1, false, P1BINS, P2I>(b, (n_build + tb - 1) / tb, 0,
+                                                "k_fscatter_build", st))
+    return rc;
+  return p2_launch<2, true, P1BINS, P2RI2>(p, (n_probe + tp - 1) / tp, 0, "k_fscatter_probe", st);
+}
+
+// The second pass of one side into sub-partitions.  counted: per-segment
+// histograms and a scan give every sub-partition's exact start (rows
+// contiguous; beg = start2, end = start2 + 1); else regions of cap2 rows
+// (beg = their starts, end = the cursors after the scatter; an overflow
+// raises ovf[1]).
+int second_pass(const JaLayout& l, int side, bool counted, long long cap2, int B, int logB2,
+                int logS, const long long* hcnt, const long long* d_pstart,
+                const long long* d_pcnt, const unsigned long long** beg,
+                const unsigned long long** end, cudaStream_t st) {
+  const long long S = (long long)B << logB2;
+  unsigned long long* cur = l.cur2 + side * l.s_max;
+  unsigned long long* start = l.start2 + side * (l.s_max + 1);
   const int sms = sm_count();
-  unsigned long long* start[2] = {l.start2, l.start2 + l.s_max + 1};
-  SegArgs g[2];
-  for (int side = 0; side < 2; ++side) {
-    // the segments, from the partition rows on the host
+  if (counted) {
     std::vector<int2> seg;
     std::vector<int> pseg((size_t)B + 1);
     for (int p = 0; p < B; ++p) {
       pseg[p] = (int)seg.size();
-      const long long n = hc[(size_t)side * B + p];
-      for (long long j = 0; j * P2SEG < n; ++j) seg.push_back(make_int2(p, (int)j));
+      for (long long j = 0; j * P2SEG < hcnt[p]; ++j) seg.push_back(make_int2(p, (int)j));
     }
     pseg[B] = (int)seg.size();
     if ((long long)seg.size() > l.nseg_max[side])
@@ -1707,17 +2023,12 @@ int join_smem(const JaLayout& l, int B, int logB, const long long* hc, long long
                               cudaMemcpyHostToDevice, st));
     PF_CUDA(cudaMemcpyAsync(l.pseg2[side], pseg.data(), pseg.size() * sizeof(int),
                             cudaMemcpyHostToDevice, st));
-    g[side].seg = l.seg2[side];
-    g[side].nseg = (int)seg.size();
-    g[side].pstart = l.start + (size_t)side * B;
-    g[side].pcnt = l.cnt + (size_t)side * B;
-    g[side].logS = logS;
-    g[side].logB2 = logB2;
-    const long long* keys = side ? l.pfk : l.pkey;
-    if (g[side].nseg) {
+    SegArgs g{l.seg2[side], (int)seg.size(), d_pstart, d_pcnt, logS, logB2};
+    if (g.nseg) {
       PF_KERNEL("k_p2_hist", st);
-      k_p2_hist<<<(unsigned)std::min<long long>(g[side].nseg, sms * 4LL), P2T, 0, st>>>(
-          keys, g[side], l.hist2[side]);
+      const unsigned grid = (unsigned)std::min<long long>(g.nseg, sms * 4LL);
+      if (side) k_p2_hist<true><<<grid, P2T, 0, st>>>(nullptr, l.prec, g, l.hist2[side]);
+      else k_p2_hist<false><<<grid, P2T, 0, st>>>(l.pkey, nullptr, g, l.hist2[side]);
     }
     PF_LAUNCH("k_p2_hist");
     {
@@ -1726,65 +2037,145 @@ int join_smem(const JaLayout& l, int B, int logB, const long long* hc, long long
           l.hist2[side], l.pseg2[side], (int)S, logB2, l.tot2 + side * l.s_max);
     }
     PF_LAUNCH("k_p2_colsum");
-    if (int rc = scan_i64(l.tot2 + side * l.s_max, (long long*)start[side], S, false,
-                          (long long*)start[side] + S, l.scan2, st))
+    if (int rc = scan_i64(l.tot2 + side * l.s_max, (long long*)start, S, false,
+                          (long long*)start + S, l.scan2, st))
       return rc;
-    PF_CUDA(cudaMemcpyAsync(l.cur2 + side * l.s_max, start[side], S * sizeof(unsigned long long),
-                            cudaMemcpyDeviceToDevice, st));
+    PF_CUDA(cudaMemcpyAsync(cur, start, S * sizeof(unsigned long long), cudaMemcpyDeviceToDevice,
+                            st));
+    *beg = start;
+    *end = start + 1;
+  } else {
+    {
+      PF_KERNEL("k_region_starts", st);
+      k_region_starts<<<(unsigned)std::min<long long>((S + 255) / 256, sms * 8LL), 256, 0, st>>>(
+          cur, l.beg2 + side * l.s_max, S, cap2);
+    }
+    PF_LAUNCH("k_region_starts");
+    *beg = l.beg2 + side * l.s_max;
+    *end = cur;
   }
-  {
-    const size_t sb = sizeof(P2Smem<int>), sp = sizeof(P2Smem<long long>);
-    if (int rc = opt_in_smem((const void*)k_p2_scatter<int, 0>, sb)) return rc;
-    if (int rc = opt_in_smem((const void*)k_p2_scatter<long long, 0>, sp)) return rc;
-    int ob = 0, op = 0;
-    PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ob, k_p2_scatter<int, 0>, P2T, sb));
-    PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&op, k_p2_scatter<long long, 0>, P2T, sp));
-    const unsigned gb = (unsigned)std::max<long long>(
-        1, std::min<long long>((n_build + P2TILE - 1) / P2TILE, (long long)std::max(1, ob) * sms));
-    const unsigned gp = (unsigned)std::max<long long>(
-        1, std::min<long long>((n_probe + P2TILE - 1) / P2TILE, (long long)std::max(1, op) * sms));
-    PF_KERNEL("k_p2_scatter", st);
-    k_p2_scatter<int, 0><<<gb, P2T, sb, st>>>(l.pkey, l.pgrp, nullptr, 0, n_build, logS, logB2, l.cur2, l.pkey2,
-                                           l.pgrp2);
-    k_p2_scatter<long long, 0><<<gp, P2T, sp, st>>>(l.pfk, l.pval, nullptr, 0, n_probe, logS, logB2,
-                                                 l.cur2 + l.s_max, l.pfk2, l.pval2);
+  // tiles partition by partition
+  std::vector<int> ts((size_t)B + 1);
+  long long nt = 0;
+  for (int p = 0; p < B; ++p) {
+    ts[p] = (int)nt;
+    nt += (hcnt[p] + P2TILE - 1) / P2TILE;
   }
-  PF_LAUNCH("k_p2_scatter");
-  unsigned long long* start_b = start[0];
-  unsigned long long* start_p = start[1];
-  SJArgs a{};
-  a.bkey = l.pkey2;
-  a.bgrp = l.pgrp2;
-  a.pfk = l.pfk2;
-  a.pval = l.pval2;
-  a.bstart = start_b;
-  a.pstart = start_p;
-  a.S = S;
+  ts[B] = (int)nt;
+  if (nt >= INT_MAX) return fail(PF_EINVAL, "join_aggregate: too many second-pass tiles");
+  PF_CUDA(cudaMemcpyAsync(l.tstart[side], ts.data(), ts.size() * sizeof(int),
+                          cudaMemcpyHostToDevice, st));
+  P2Args a{};
+  a.pstart = d_pstart;
+  a.pcnt = d_pcnt;
+  a.tstart = l.tstart[side];
+  a.B = B;
   a.logS = logS;
-  a.group_min = group_min;
-  a.n_groups = n_groups;
-  a.slab = l.slab;
-  a.stats = (unsigned long long*)stats_out;
-  a.counter = l.sj_counter;
-  PF_CUDA(cudaMemsetAsync(l.sj_counter, 0, sizeof(unsigned long long), st));
-  {
-    const size_t smem = sizeof(SJSmem);
-    if (int rc = opt_in_smem((const void*)k_sjoin, smem)) return rc;
-    int per_sm = 0;
-    PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sjoin, SJT, smem));
-    PF_KERNEL("k_sjoin", st);
-    k_sjoin<<<std::max(1, per_sm) * sms, SJT, smem, st>>>(a);
+  a.logB2 = logB2;
+  a.cursor = cur;
+  a.cap = counted ? 0 : cap2;
+  a.ovf = l.ovf + 1;
+  const size_t extra = ((size_t)B + 1) * sizeof(int);
+  if (side) {
+    a.rec = l.prec;
+    a.rec_out = l.prec2;
+    return p2_launch<0, true, P2BINS, P2I>(a, nt, extra, "k_p2_scatter", st);
   }
-  PF_LAUNCH("k_sjoin");
-  {
-    PF_KERNEL("k_split", st);
-    k_split<<<(unsigned)std::max<long long>(1, std::min<long long>((n_groups + 255) / 256, sms * 8LL)),
-              256, 0, st>>>(l.slab, n_groups, (long long*)sum_out, (long long*)count_out);
-  }
-  PF_LAUNCH("k_split");
-  return ok();
+  a.key = l.pkey;
+  a.val = l.pgrp;
+  a.key_out = l.pkey2;
+  a.val_out = l.pgrp2;
+  return p2_launch<0, false, P2BINS, P2I>(a, nt, extra, "k_p2_scatter", st);
 }
 
+// The shared-memory path after the first pass (counts on the host, hc[2B],
+// partitions at d_pstart): the second radix pass into sub-partitions of
+// about SJ_TARGET build rows, the join per sub-partition, the slab split.
+// A side whose regions would not fit its buffer, or every side after an
+// overflow, takes the counted second pass.  Keys are mix64 hashes here.
+int join_smem(const JaLayout& l, int B, int logB, const long long* hc, long long n_build,
+              long long n_probe, long long group_min, long long n_groups, int64_t* sum_out,
+              int64_t* count_out, int64_t* stats_out, long long* hstage, cudaStream_t st) {
+  (void)n_build;
+  (void)n_probe;
+  long long maxp[2] = {0, 0};
+  for (int side = 0; side < 2; ++side)
+    for (int p = 0; p < B; ++p) maxp[side] = std::max(maxp[side], hc[(size_t)side * B + p]);
+  int logB2 = 0;
+  while ((maxp[0] >> logB2) > SJ_TARGET && logB2 < P2MAXLOG &&
+         ((long long)B << (logB2 + 1)) <= l.s_max)
+    ++logB2;
+  const int logS = logB + logB2;
+  const long long S = 1LL << logS;
+  const int sms = sm_count();
+  const char* force = getenv("PF_COUNTED");
+  bool counted[2];
+  long long cap2[2];
+  for (int side = 0; side < 2; ++side) {
+    cap2[side] = region_rows((double)maxp[side] / (double)(1LL << logB2));
+    counted[side] = (force && force[0] == '1') || S * cap2[side] > l.rows2[side];
+  }
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    PF_CUDA(cudaMemsetAsync(l.ovf + 1, 0, sizeof(unsigned long long), st));
+    const unsigned long long *bbeg, *bend, *pbeg, *pend;
+    if (int rc = second_pass(l, 0, counted[0], cap2[0], B, logB2, logS, hc, l.pstart,
+                             l.pstart + 2 * B, &bbeg, &bend, st))
+      return rc;
+    if (int rc = second_pass(l, 1, counted[1], cap2[1], B, logB2, logS, hc + B, l.pstart + B,
+                             l.pstart + 3 * B, &pbeg, &pend, st))
+      return rc;
+    SJArgs a{};
+    a.bkey = l.pkey2;
+    a.bgrp = l.pgrp2;
+    a.prec = l.prec2;
+    a.bbeg = bbeg;
+    a.bend = bend;
+    a.pbeg = pbeg;
+    a.pend = pend;
+    a.S = S;
+    a.logS = logS;
+    a.group_min = group_min;
+    a.n_groups = n_groups;
+    a.slab = l.slab;
+    a.stats = (unsigned long long*)stats_out;
+    a.counter = l.sj_counter;
+    a.ovf = l.ovf + 1;
+    PF_CUDA(cudaMemsetAsync(l.sj_counter, 0, sizeof(unsigned long long), st));
+    const char* fpe = getenv("PF_SJ_FP");
+    if (fpe ? fpe[0] == '1' : PF_SJ_FP_DEFAULT) {
+      const size_t smem = sizeof(SJFSmem);
+      if (int rc = opt_in_smem((const void*)k_sjoin_fp, smem)) return rc;
+      int per_sm = 0;
+      PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sjoin_fp, SJF_T, smem));
+      PF_KERNEL("k_sjoin", st);
+      k_sjoin_fp<<<std::max(1, per_sm) * sms, SJF_T, smem, st>>>(a);
+    } else {
+      const size_t smem = sizeof(SJSmem);
+      if (int rc = opt_in_smem((const void*)k_sjoin, smem)) return rc;
+      int per_sm = 0;
+      PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sjoin, SJT, smem));
+      PF_KERNEL("k_sjoin", st);
+      k_sjoin<<<std::max(1, per_sm) * sms, SJT, smem, st>>>(a);
+    }
+    PF_LAUNCH("k_sjoin");
+    {
+      PF_KERNEL("k_split", st);
+      k_split<<<(unsigned)std::max<long long>(
+                    1, std::min<long long>((n_groups + 255) / 256, sms * 8LL)),
+                256, 0, st>>>(l.slab, n_groups, (long long*)sum_out, (long long*)count_out);
+    }
+    PF_LAUNCH("k_split");
+    g_counted_passes = (g_counted_passes & 1) | (counted[0] || counted[1] ? 2 : 0);
+    if (counted[0] && counted[1]) return ok();
+    // regions: whether one overflowed (then nothing was joined)
+    PF_CUDA(cudaMemcpyAsync(hstage, l.ovf + 1, sizeof(unsigned long long),
+                            cudaMemcpyDeviceToHost, st));
+    if (int rc = wait_stream(st)) return rc;
+    if (!hstage[0]) return ok();
+    counted[0] = counted[1] = true;
+  }
+  return fail(PF_ECUDA, "join_aggregate: the counted second pass overflowed");
+}
 }  // namespace
 }  // namespace pf
 
@@ -1797,6 +2188,8 @@ extern "C" int pf_join_aggregate_pick_b(int64_t n_build, int64_t n_probe) {
   while (b < FB_MAX && n_build / b > target) b <<= 1;
   return (int)b;
 }
+
+extern "C" int pf_join_aggregate_counted_passes(void) { return g_counted_passes; }
 
 extern "C" size_t pf_join_aggregate_workspace(int64_t n_build, int64_t n_probe, int B,
                                               int64_t n_groups) {
@@ -1835,67 +2228,88 @@ extern "C" int pf_join_aggregate(const int64_t* build_key, const int32_t* build_
   }
   PF_CUDA(cudaMemsetAsync(l.slab, 0, 2 * n_groups * sizeof(unsigned long long), st));
 
-  // 1-2: histograms and offsets of both sides
+  long long* hc = pinned_counts(2 * (size_t)B + 8);
+  if (!hc) return fail(PF_ECUDA, "join_aggregate: no pinned staging buffer");
+  const int sms = sm_count();
+  if (join_path_smem()) {
+    // 1: the first pass into regions of cap1 rows a bucket, from their starts
+    const char* force = getenv("PF_COUNTED");
+    bool counted = force && force[0] == '1';
+    std::vector<long long> part(4 * (size_t)B);  // starts, then rows, of both sides
+    if (!counted) {
+      for (int side = 0; side < 2; ++side) {
+        PF_KERNEL("k_region_starts", st);
+        k_region_starts<<<(unsigned)std::max(1, (B + 255) / 256), 256, 0, st>>>(
+            l.cur1 + (size_t)side * B, nullptr, B, l.cap1[side]);
+      }
+      PF_LAUNCH("k_region_starts");
+      PF_CUDA(cudaMemsetAsync(l.ovf, 0, sizeof(unsigned long long), st));
+      if (int rc = first_pass(build_key, build_group, n_build, probe_fk, probe_price, probe_disc,
+                              scale, n_probe, logB, B, l.cap1, l, st))
+        return rc;
+      // the cursors are the buckets' ends
+      PF_CUDA(cudaMemcpyAsync(hc, l.cur1, 2 * B * sizeof(long long), cudaMemcpyDeviceToHost, st));
+      PF_CUDA(cudaMemcpyAsync(hc + 2 * B, l.ovf, sizeof(long long), cudaMemcpyDeviceToHost, st));
+      if (int rc = wait_stream(st)) return rc;
+      counted = hc[2 * B] != 0;
+      if (!counted)
+        for (int side = 0; side < 2; ++side)
+          for (int p = 0; p < B; ++p) {
+            const size_t i = (size_t)side * B + p;
+            part[i] = p * l.cap1[side];
+            part[2 * (size_t)B + i] = hc[i] - part[i];
+          }
+    }
+    if (counted) {
+      // a bucket overflowed its region (or counting was asked for): count
+      // first, then scatter from the exact starts
+      const long long none[2] = {0, 0};
+      cudaEvent_t ev;
+      if (int rc = count_buckets(build_key, n_build, probe_fk, n_probe, logB, B, l, hc, &ev, st))
+        return rc;
+      PF_CUDA(cudaMemcpyAsync(l.cur1, l.start, 2 * B * sizeof(long long),
+                              cudaMemcpyDeviceToDevice, st));
+      if (int rc = first_pass(build_key, build_group, n_build, probe_fk, probe_price, probe_disc,
+                              scale, n_probe, logB, B, none, l, st))
+        return rc;
+      if (int rc = wait_event(ev)) return rc;
+      for (int side = 0; side < 2; ++side) {
+        long long run = 0;
+        for (int p = 0; p < B; ++p) {
+          const size_t i = (size_t)side * B + p;
+          part[i] = run;
+          part[2 * (size_t)B + i] = hc[i];
+          run += hc[i];
+        }
+      }
+    }
+    g_counted_passes = counted ? 1 : 0;
+    // pageable source: the copy takes the data before it returns
+    PF_CUDA(cudaMemcpyAsync(l.pstart, part.data(), part.size() * sizeof(long long),
+                            cudaMemcpyHostToDevice, st));
+    return join_smem(l, B, logB, part.data() + 2 * (size_t)B, n_build, n_probe, group_min,
+                     n_groups, sum_out, count_out, stats_out, hc, st);
+  }
+
+  // the round path: counts, then the first pass, queued while the host waits
+  // for the counts
+  g_counted_passes = 1;
+  cudaEvent_t ev;
+  if (int rc = count_buckets(build_key, n_build, probe_fk, n_probe, logB, B, l, hc, &ev, st))
+    return rc;
   long long chunk_b, chunk_p;
   int nch_b, nch_p;
   chunking(n_build, &chunk_b, &nch_b);
   chunking(n_probe, &chunk_p, &nch_p);
-  const size_t hsm = (size_t)B * sizeof(int);
-  {
-    PF_KERNEL("k_fhist", st);
-    k_fhist<<<nch_b, FT, hsm, st>>>((const long long*)build_key, n_build, chunk_b, logB, B, l.hist_b);
-  }
-  {
-    PF_KERNEL("k_fhist", st);
-    k_fhist<<<nch_p, FT, hsm, st>>>((const long long*)probe_fk, n_probe, chunk_p, logB, B, l.hist_p);
-  }
-  PF_LAUNCH("k_fhist");
-  {
-    PF_KERNEL("k_fscan", st);
-    k_fscan<<<(B + 31) / 32, FT, 0, st>>>(l.hist_b, nch_b, B, l.cnt);
-  }
-  {
-    PF_KERNEL("k_fscan", st);
-    k_fscan<<<(B + 31) / 32, FT, 0, st>>>(l.hist_p, nch_p, B, l.cnt + B);
-  }
-  PF_LAUNCH("k_fscan");
-  PF_CUDA(cudaMemcpyAsync(l.start, l.cnt, 2 * B * sizeof(long long), cudaMemcpyDeviceToDevice, st));
-  {
-    PF_KERNEL("k_scan_counts", st);
-    k_scan_counts<<<1, 1024, 0, st>>>(l.start, B, l.total, nullptr);
-  }
-  {
-    PF_KERNEL("k_scan_counts", st);
-    k_scan_counts<<<1, 1024, 0, st>>>(l.start + B, B, l.total + 1, nullptr);
-  }
-  PF_LAUNCH("k_scan_counts");
-  long long* hc = pinned_counts(2 * (size_t)B);
-  if (!hc) return fail(PF_ECUDA, "join_aggregate: no pinned staging buffer");
-  PF_CUDA(cudaMemcpyAsync(hc, l.cnt, 2 * B * sizeof(long long), cudaMemcpyDeviceToHost, st));
-  cudaEvent_t ev;
-  if (int rc = record_event(st, &ev)) return rc;
-
-  // 3: the scatters, queued while the host waits for the counts
   const bool tma = aligned16(build_key) && aligned16(build_group) && aligned16(probe_fk) &&
                    aligned16(probe_price) && (!probe_disc || aligned16(probe_disc)) &&
                    getenv("PF_NO_TMA") == nullptr;
-  const bool smem_path = join_path_smem() != 0;
-  const char* fe = getenv("PF_FIRST_TILE");
-  const bool tile_first = smem_path && B <= P2BINS && (fe ? fe[0] != '0' : PF_FIRST_TILE);
-  if (int rc = tile_first ? first_pass_tile(build_key, build_group, n_build, probe_fk, probe_price,
-                                            probe_disc, scale, n_probe, logB, B, l, st)
-               : smem_path ? fscatter_both<true>(tma, build_key, build_group, n_build, probe_fk,
-                                                probe_price, probe_disc, scale, n_probe, chunk_b,
-                                                nch_b, chunk_p, nch_p, logB, B, l, stats_out, st)
-                         : fscatter_both<false>(tma, build_key, build_group, n_build, probe_fk,
-                                                 probe_price, probe_disc, scale, n_probe, chunk_b,
-                                                 nch_b, chunk_p, nch_p, logB, B, l, stats_out, st))
+  if (int rc = fscatter_rounds(tma, build_key, build_group, n_build, probe_fk, probe_price,
+                               probe_disc, scale, n_probe, chunk_b, nch_b, chunk_p, nch_p, logB,
+                               B, l, stats_out, st))
     return rc;
   PF_LAUNCH("k_fscatter");
   if (int rc = wait_event(ev)) return rc;
-  if (join_path_smem())
-    return join_smem(l, B, logB, hc, n_build, n_probe, group_min, n_groups, sum_out, count_out,
-                     stats_out, st);
 
   // 4: plan the rounds from the counts
   const long long cap_rows = l.table_slots / 2;
@@ -1972,7 +2386,6 @@ extern "C" int pf_join_aggregate(const int64_t* build_key, const int32_t* build_
     x.table = l.table + (r & 1) * l.table_slots;
     return x;
   };
-  const int sms = sm_count();
   // launch k: probe round k - 1 and build round k
   for (long long k = 0; k <= (long long)rounds.size(); ++k) {
     RoundArgs pa = round_args(k - 1), ba = round_args(k);

@@ -90,10 +90,22 @@ def test_slab_large_sum_is_exact_int64():
 
 # ---- the fused join -> group-by ---------------------------------------------------
 
-@pytest.fixture(params=["rounds", "smem"])
+@pytest.fixture(params=["rounds", "smem", "smem-counted"])
 def join_path(request, monkeypatch):
-    monkeypatch.setenv("PF_JOIN_PATH", request.param)
+    """The round path, the shared-memory path (regions sized from the
+    expected rows, counted again on an overflow) and the shared-memory path
+    with both radix passes counted first."""
+    monkeypatch.setenv("PF_JOIN_PATH", request.param.split("-")[0])
+    if request.param.endswith("counted"):
+        monkeypatch.setenv("PF_COUNTED", "1")
+    else:
+        monkeypatch.delenv("PF_COUNTED", raising=False)
     return request.param
+
+
+def _counted_passes():
+    from pageflow_b200 import _native
+    return _native.lib().pf_join_aggregate_counted_passes()
 
 
 def _oracle_groups(bkey, bgrp, fk, price, disc, group_min, n_groups, scale=100):
@@ -309,3 +321,17 @@ def test_skewed_probe_keys(B, join_path):
     assert plan.read_stats().matched == want[3]
     top = torch.bincount(ranks, minlength=nb).max().item()
     assert top > np_ // 50                            # the hottest key takes > 2% of the rows
+    if join_path == "smem":
+        # the hot keys crowd their (sub-)buckets past the regions: the pass
+        # that overflowed ran again, counted
+        assert _counted_passes() & (1 if B > 1 else 2)
+
+
+def test_uniform_keys_fill_the_regions_without_counting(join_path):
+    w = datagen.scaled(datagen.SCALE, 1 / 300)   # 500K x 2M, 5000 groups
+    bkey, bgrp = datagen.gen_build(w, "cuda")
+    fk, price, disc = datagen.gen_probe(w, "cuda")
+    want = _oracle_groups(bkey, bgrp, fk, price, disc, 0, w.n_groups)
+    plan = JoinAggregate(w.n_build, w.n_probe, 0, w.n_groups, "cuda", B=64)
+    _assert_groups(plan.run(bkey, bgrp, fk, price, disc), want)
+    assert {"rounds": 1, "smem": 0, "smem-counted": 3}[join_path] == _counted_passes()

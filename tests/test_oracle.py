@@ -140,3 +140,25 @@ def test_expand_oracle():
     cs, cr = oracle.expand(sorted_ids, start, length)
     assert cs.tolist() == [100, 101, 105, 106, 107, 110]
     assert cr.tolist() == [0, 0, 2, 2, 2, 3]
+
+
+def test_plain_forms_aggregation_is_the_references():
+    """The GPU plain form's aggregation steps (oracle/plain_form.aggregate:
+    KeyedAggregate.pass1 per morsel, buckets, reduce_tick_slice per round),
+    run on the CPU over the small workload's joined rows, give the
+    reference's own result (config0.npz, made by its _sort_search_pairs,
+    KeyedAggregate.pass1 and reduce_tick_slice)."""
+    import torch
+
+    import oracle
+    from oracle import plain_form
+    g = load("config0.npz")
+    bkey, bgrp = oracle.gen_build(0, 250_000, 25)
+    fk, price, disc = oracle.gen_probe(0, 0, 250_000, 0, 1_000_000)
+    bi, pi = oracle.join_unique([bkey], [fk])
+    keys, sums, counts = plain_form.aggregate(torch.from_numpy(bgrp[bi]),
+                                              torch.from_numpy(price[pi]),
+                                              torch.from_numpy(disc[pi]), 100)
+    assert np.array_equal(keys.numpy(), g["groups"])
+    assert np.array_equal(sums.numpy(), g["sums"])
+    assert np.array_equal(counts.numpy(), g["counts"])
