@@ -292,6 +292,15 @@ def run_ours(args, w, world, rank, local_rank):
     keys, sums, counts = step()
     n_groups_out = int(keys.numel())
     matched = plan.read_stats().matched
+    # the autotuner's pick (made on the first warm-up call) and its timings
+    tuning = None
+    if plan.tuning is not None:
+        t = plan.tuning
+        tuning = {"choice": {"B": t.choice.B, "table": t.choice.table,
+                             "sub_rows": t.choice.sub_rows},
+                  "cached": t.cached, "candidate_ms": t.times_ms}
+    elif plan.knobs is None:
+        tuning = {"off": "a PF_* override or an explicit --B fixes the configuration"}
     # rounds of the plan (for the per-launch figures)
 
     gpu_id = None
@@ -396,7 +405,8 @@ def run_ours(args, w, world, rank, local_rank):
                        "groups": w.n_groups, "fanout_B": plan.B, "parallelism":
                        "replicas" if world > 1 else "single",
                        "l2": "inputs (16 B/row build, 24 B/row probe) exceed L2; no flush",
-                       "groups_out": n_groups_out, "matched_probe_rows": matched},
+                       "groups_out": n_groups_out, "matched_probe_rows": matched,
+                       "autotune": tuning},
             "roofline": roofline, "step_roofline": step_roofline,
             "kernels": kernels,
             "e2e": e2e, "cpu_baseline": cpu, "plain_form": plain, "clocks": clocks,

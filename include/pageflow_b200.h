@@ -125,13 +125,19 @@ int pf_join_unique_hash(const int64_t* build0, const int64_t* build1, int64_t n_
  * No counterpart in the reference.  pf_join_unique_hash for callers that may
  * not allocate: no workspace argument and no device allocation by the
  * library; its scratch is one fixed device array of
- * PF_UH_STATIC_SCRATCH_BYTES (8 MiB + 64 KiB) inside the library, enough for
- * 524288 build rows with 1048576 probe rows (the table takes 8 bytes per
- * build row, the partners 4 bytes per probe row).  Larger calls return PF_EINVAL before anything is queued.  The match
+ * PF_UH_STATIC_SCRATCH_BYTES (8 MiB + 64 KiB) inside the library.  A call
+ * fits when 8 * n_build + 4 * n_probe bytes, plus 8 bytes per 4096 probe
+ * rows of block counts, stay within it: 524288 build rows with 1048576
+ * probe rows is one such call, and so is 1000000 build rows with 10 probe
+ * rows.  Larger calls return PF_EINVAL before anything is queued.  The match
  * count goes to match_count (device int64[1]) on the stream; nothing waits.
  * The first call on a device, with that device current, sets the scratch up
  * (looks up its device address, loading the library's module there); make
- * it before any stream capture.  The scratch is shared per device: calls
+ * it before any stream capture.  Every call takes the device that is
+ * current when it is made, so `stream` must belong to that device.  The
+ * address is kept for the life of the process: after cudaDeviceReset it
+ * names memory of the destroyed context, so do not call this entry point on
+ * a device after resetting it.  The scratch is shared per device: calls
  * that overlap on one device (two streams, two host threads) race.
  */
 #define PF_UH_STATIC_SCRATCH_BYTES ((8u << 20) + (64u << 10))
@@ -155,6 +161,28 @@ int pf_gather(const void* const* cols_in, void* const* cols_out, const int* row_
               const int* elem_bytes, const uint64_t* null_elem, int ncols, const int64_t* idx,
               int64_t n, int64_t n_src, int allow_null, int64_t null_idx, int64_t* bad,
               void* stream);
+
+/*
+ * Late materialization with zero copy: the same gather from columns held in
+ * pinned host memory as segments, read in place over the host link (the
+ * reference's zero_copy_rearrange_kernel, IO/zero_copy_reader.cu:89-118, with
+ * an error count where it traps).  Segment s of every column holds rows
+ * [seg_rows[s], seg_rows[s + 1]) (host int64, ascending, nseg + 1 of them,
+ * nseg <= 1024); seg_ptrs[c * nseg + s] is column c's segment s (pinned host
+ * memory, cudaHostAlloc or registered).  Output row i of column c is row
+ * idx[i] + base; an index equal to null_idx (with allow_null) gives a row of
+ * null_elem[c] elements, an index outside the segments that row too, counted
+ * in bad[0] (device int64, added to) and never read.  With order (device
+ * int64[n], a permutation of [0, n), e.g. the argsort of idx), output rows
+ * are taken in that order, so neighbouring threads read neighbouring host
+ * rows.  Workspace: pf_gather_segments_workspace(ncols, nseg).  Queued only.
+ */
+size_t pf_gather_segments_workspace(int ncols, int nseg);
+int pf_gather_segments(void* const* seg_ptrs, const int64_t* seg_rows, int nseg, int64_t base,
+                       int ncols, const int* row_bytes, const int* elem_bytes,
+                       const uint64_t* null_elem, const int64_t* idx, const int64_t* order,
+                       int64_t n, int allow_null, int64_t null_idx, void* const* cols_out,
+                       int64_t* bad, void* workspace, size_t workspace_bytes, void* stream);
 
 /* Residual operators of a semi/anti summary, as build.v OP probe.v. */
 #define PF_OP_NONE 0
@@ -252,6 +280,78 @@ int pf_join_aggregate(const int64_t* build_key, const int32_t* build_group, int6
                       const int64_t* probe_disc, int64_t scale, int64_t n_probe, int B,
                       int64_t group_min, int64_t n_groups, int64_t* sum_out, int64_t* count_out,
                       int64_t* stats_out, void* workspace, size_t workspace_bytes, void* stream);
+/*
+ * The run-time choices of a fused join + group-by, the autotuner's knobs
+ * beside the fan-out B (pageflow_b200/autotune.py times candidates on a
+ * shape's first call and caches the fastest).  No counterpart in the
+ * reference, whose fan-out comes from its partition-count rule alone
+ * (operators/partitions.py:54-85).
+ *   path      0: the shared-memory join (second radix pass, a table per
+ *             sub-partition in shared memory); 1: L2 rounds (one radix pass,
+ *             tables in L2; a smaller workspace)
+ *   table     shared-memory join: 0 a table of 8-byte hash slots, 1 4-byte
+ *             fingerprinted slots with the build hashes and cells by row
+ *   sub_rows  build rows a sub-partition aims at (0: 1365); fewer rows, more
+ *             sub-partitions in the second radix pass
+ *   counted   1: both radix passes count their rows before they scatter
+ *             (else only a pass whose regions overflowed)
+ * With knobs = NULL the defaults apply (overridden, for sweeps, by
+ * PF_JOIN_PATH=rounds|smem, PF_SJ_FP, PF_SJ_TARGET and PF_COUNTED).  The
+ * workspace depends on the knobs: query it with the same ones.
+ */
+typedef struct pf_join_knobs {
+  int path;
+  int table;
+  int sub_rows;
+  int counted;
+} pf_join_knobs;
+size_t pf_join_aggregate_workspace_ex(int64_t n_build, int64_t n_probe, int B, int64_t n_groups,
+                                      const pf_join_knobs* knobs);
+int pf_join_aggregate_ex(const int64_t* build_key, const int32_t* build_group, int64_t n_build,
+                         const int64_t* probe_fk, const int64_t* probe_price,
+                         const int64_t* probe_disc, int64_t scale, int64_t n_probe, int B,
+                         int64_t group_min, int64_t n_groups, int64_t* sum_out,
+                         int64_t* count_out, int64_t* stats_out, const pf_join_knobs* knobs,
+                         void* workspace, size_t workspace_bytes, void* stream);
+/*
+ * The fused join + group-by sharded over ranks, in its two rank-local
+ * phases (no counterpart in the reference, which runs on one GPU; the
+ * exchange between them is the caller's, e.g. NCCL all-to-alls):
+ *
+ * pf_join_partition: a rank's rows hashed and radix-partitioned into B
+ * buckets (B a power of two <= 4096; bucket = top log2(B) bits of
+ * mix64(key)), counted first so that every bucket is contiguous, in bucket
+ * order: build rows as build_hash_out[n_build] (mix64 of the key) and
+ * build_group_out[n_build], probe rows as probe_rec_out[2 * n_probe]
+ * records {mix64(fk), price * (scale - disc)} (price when disc is NULL).
+ * host_counts (host int64[2B]): each bucket's build rows, then its probe
+ * rows.  Waits once, for the counts.
+ *
+ * pf_join_aggregate_buckets: the second radix pass and the join over nbk
+ * buckets a rank holds, each bucket's rows contiguous and the buckets one
+ * after another on each side (counts: host int64[2 * nbk], build rows of
+ * every bucket, then probe rows; every row of a bucket shares the top logB
+ * bits of its hash), into sum_out / count_out [n_groups] over [group_min,
+ * group_min + n_groups) and stats_out as pf_join_aggregate's.  Knobs as
+ * pf_join_aggregate_ex's (the shared-memory join only).  Adding the ranks'
+ * slabs gives the join's result.  Waits at the end unless both sides'
+ * second pass was counted.
+ */
+size_t pf_join_partition_workspace(int64_t n_build, int64_t n_probe, int B);
+int pf_join_partition(const int64_t* build_key, const int32_t* build_group, int64_t n_build,
+                      const int64_t* probe_fk, const int64_t* probe_price,
+                      const int64_t* probe_disc, int64_t scale, int64_t n_probe, int B,
+                      int64_t* build_hash_out, int32_t* build_group_out, int64_t* probe_rec_out,
+                      int64_t* host_counts, void* workspace, size_t workspace_bytes,
+                      void* stream);
+size_t pf_join_aggregate_buckets_workspace(const int64_t* counts, int nbk, int64_t n_groups,
+                                           const pf_join_knobs* knobs);
+int pf_join_aggregate_buckets(const int64_t* build_hash, const int32_t* build_group,
+                              const int64_t* probe_rec, const int64_t* counts, int nbk,
+                              int logB, int64_t group_min, int64_t n_groups, int64_t* sum_out,
+                              int64_t* count_out, int64_t* stats_out,
+                              const pf_join_knobs* knobs, void* workspace,
+                              size_t workspace_bytes, void* stream);
 /* The fan-out the autotuner seeds pf_join_aggregate with for these sizes. */
 int pf_join_aggregate_pick_b(int64_t n_build, int64_t n_probe);
 /*

@@ -15,6 +15,12 @@ import os
 LIB_PATH = Path(os.environ.get("PAGEFLOW_B200_LIB",
                                Path(__file__).resolve().parent / "libpageflow_b200.so"))
 
+class JoinKnobs(ctypes.Structure):
+    """pf_join_knobs: the run-time choices of a fused join + group-by."""
+    _fields_ = [("path", ctypes.c_int), ("table", ctypes.c_int), ("sub_rows", ctypes.c_int),
+                ("counted", ctypes.c_int)]
+
+
 PF_OK = 0
 PF_EINVAL = -1
 PF_ECUDA = -2
@@ -45,6 +51,9 @@ _SIGS = {
                                    _vp, _vp, _sz, _vp]),
     "pf_join_unique_hash_static": (_int, [_vp, _vp, _i64, _vp, _vp, _i64, _int, _vp, _vp, _vp,
                                           _vp]),
+    "pf_gather_segments_workspace": (_sz, [_int, _int]),
+    "pf_gather_segments": (_int, [_vp, _vp, _int, _i64, _int, _vp, _vp, _vp, _vp, _vp, _i64,
+                                  _int, _i64, _vp, _vp, _vp, _sz, _vp]),
     "pf_gather": (_int, [_vp, _vp, _vp, _vp, _vp, _int, _vp, _i64, _i64, _int, _i64, _vp, _vp]),
     "pf_join_semi_anti_workspace": (_sz, [_i64, _i64, _int]),
     "pf_join_semi_anti": (_int, [_vp, _i64, _vp, _i64, _vp, _vp, _int, _int, _vp,
@@ -60,6 +69,15 @@ _SIGS = {
     "pf_join_aggregate_workspace": (_sz, [_i64, _i64, _int, _i64]),
     "pf_join_aggregate": (_int, [_vp, _vp, _i64, _vp, _vp, _vp, _i64, _i64, _int,
                                  _i64, _i64, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "pf_join_aggregate_workspace_ex": (_sz, [_i64, _i64, _int, _i64, _vp]),
+    "pf_join_aggregate_ex": (_int, [_vp, _vp, _i64, _vp, _vp, _vp, _i64, _i64, _int, _i64, _i64,
+                                    _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "pf_join_partition_workspace": (_sz, [_i64, _i64, _int]),
+    "pf_join_partition": (_int, [_vp, _vp, _i64, _vp, _vp, _vp, _i64, _i64, _int, _vp, _vp, _vp,
+                                 _vp, _vp, _sz, _vp]),
+    "pf_join_aggregate_buckets_workspace": (_sz, [_vp, _int, _i64, _vp]),
+    "pf_join_aggregate_buckets": (_int, [_vp, _vp, _vp, _vp, _int, _int, _i64, _i64, _vp, _vp,
+                                         _vp, _vp, _vp, _sz, _vp]),
     "pf_join_aggregate_pick_b": (_int, [_i64, _i64]),
     "pf_join_aggregate_counted_passes": (_int, []),
     "pf_groups_finish_workspace": (_sz, [_i64]),

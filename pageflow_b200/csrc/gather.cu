@@ -13,6 +13,7 @@
 // one such step, a thread takes several rows with all their loads issued
 // before the first store.
 #include <algorithm>
+#include <vector>
 
 #include "common.cuh"
 
@@ -185,6 +186,77 @@ __global__ void __launch_bounds__(GT) k_gather_words(GatherArgs a) {
   if ((threadIdx.x & 31) == 0 && bad && a.bad) atomicAdd(a.bad, bad);
 }
 
+
+// ---- zero copy: rows read in place from pinned host segments ----------------
+//
+// A column spread over host segments (segment s holds rows [seg_rows[s],
+// seg_rows[s + 1]) at seg[c * nseg + s], device aliases of pinned host
+// memory).  Output row i of column c is row idx[i] - base of the column read
+// over the host link; a null index gives the null row, an index outside the
+// segments the null row too, counted in bad[0] (never read).  With order,
+// thread k takes output row order[k], so that consecutive threads read
+// consecutive host rows when order sorts the indexes.
+constexpr int ZT = 256;
+constexpr int ZMAXSEG = 1024;  // segments the block's shared-memory table holds
+
+struct SegGatherArgs {
+  const unsigned char* const* seg;  // [ncols * nseg]
+  const long long* seg_rows;        // [nseg + 1] ascending
+  int nseg, ncols;
+  long long base;
+  const long long* idx;
+  const long long* order;           // or null
+  long long n;
+  long long null_idx;
+  int allow_null;
+  int row_bytes[GMAXC];
+  int esize[GMAXC];
+  unsigned long long null_elem[GMAXC];
+  unsigned char* out[GMAXC];
+  unsigned long long* bad;
+};
+
+__global__ void __launch_bounds__(ZT) k_gather_segments(SegGatherArgs a) {
+  __shared__ long long bounds[ZMAXSEG + 1];
+  for (int s = threadIdx.x; s <= a.nseg; s += ZT) bounds[s] = a.seg_rows[s];
+  __syncthreads();
+  unsigned long long bad = 0;
+  for (long long k = (long long)blockIdx.x * ZT + threadIdx.x; k < a.n;
+       k += (long long)gridDim.x * ZT) {
+    const long long i = a.order ? a.order[k] : k;
+    const long long j = a.idx[i];
+    int seg = -1;
+    long long row = 0;
+    if (!(a.allow_null && j == a.null_idx)) {
+      const long long r = j + a.base;
+      if (r >= bounds[0] && r < bounds[a.nseg]) {
+        int lo = 0, hi = a.nseg;  // bounds[lo] <= r < bounds[hi]
+        while (hi - lo > 1) {
+          const int m = (lo + hi) >> 1;
+          if (bounds[m] <= r) lo = m;
+          else hi = m;
+        }
+        seg = lo;
+        row = r - bounds[lo];
+      } else {
+        ++bad;
+      }
+    }
+    for (int c = 0; c < a.ncols; ++c) {
+      const int rb = a.row_bytes[c];
+      unsigned char* dst = a.out[c] + i * rb;
+      if (seg >= 0) {
+        const unsigned char* src = a.seg[(long long)c * a.nseg + seg] + row * rb;
+        for (int b = 0; b < rb; ++b) dst[b] = src[b];
+      } else {
+        for (int b = 0; b < rb; ++b)
+          dst[b] = (unsigned char)(a.null_elem[c] >> (8 * (b % a.esize[c])));
+      }
+    }
+  }
+  for (int o = 16; o; o >>= 1) bad += __shfl_xor_sync(FULL, bad, o);
+  if ((threadIdx.x & 31) == 0 && bad) atomicAdd(a.bad, bad);
+}
 }  // namespace
 }  // namespace pf
 
@@ -276,5 +348,89 @@ extern "C" int pf_gather(const void* const* cols_in, void* const* cols_out, cons
     }
   }
   PF_LAUNCH("k_gather");
+  return ok();
+}
+
+extern "C" size_t pf_gather_segments_workspace(int ncols, int nseg) {
+  Arena a(nullptr, 0);
+  a.take<const unsigned char*>((size_t)ncols * nseg);
+  a.take<long long>((size_t)nseg + 1);
+  return a.used + 256;
+}
+
+extern "C" int pf_gather_segments(void* const* seg_ptrs, const int64_t* seg_rows, int nseg,
+                                  int64_t base, int ncols, const int* row_bytes,
+                                  const int* elem_bytes, const uint64_t* null_elem,
+                                  const int64_t* idx, const int64_t* order, int64_t n,
+                                  int allow_null, int64_t null_idx, void* const* cols_out,
+                                  int64_t* bad, void* workspace, size_t workspace_bytes,
+                                  void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (ncols < 1 || ncols > GMAXC) return fail(PF_EINVAL, "gather_segments: 1 to %d columns", GMAXC);
+  if (nseg < 1 || nseg > ZMAXSEG)
+    return fail(PF_EINVAL, "gather_segments: 1 to %d segments, got %d", ZMAXSEG, nseg);
+  if (n < 0) return fail(PF_EINVAL, "gather_segments: negative rows");
+  if (!bad || !seg_ptrs || !seg_rows) return fail(PF_EINVAL, "gather_segments: null argument");
+  for (int s = 0; s < nseg; ++s)
+    if (seg_rows[s + 1] < seg_rows[s])
+      return fail(PF_EINVAL, "gather_segments: segment rows must ascend");
+  Arena ar(workspace, workspace_bytes);
+  const unsigned char** dseg = ar.take<const unsigned char*>((size_t)ncols * nseg);
+  long long* drows = ar.take<long long>((size_t)nseg + 1);
+  if (!workspace || !ar.fits())
+    return fail(PF_ENOSPACE, "gather_segments: workspace of %zu bytes, %zu needed",
+                workspace_bytes, ar.used);
+  SegGatherArgs a{};
+  for (int c = 0; c < ncols; ++c) {
+    const int e = elem_bytes[c];
+    if (row_bytes[c] < 1 || (e != 1 && e != 2 && e != 4 && e != 8) || row_bytes[c] % e)
+      return fail(PF_EINVAL, "gather_segments: column %d: %d-byte rows of %d-byte elements", c,
+                  row_bytes[c], e);
+    if (n > 0 && !cols_out[c]) return fail(PF_EINVAL, "gather_segments: column %d is null", c);
+    a.row_bytes[c] = row_bytes[c];
+    a.esize[c] = e;
+    a.null_elem[c] = null_elem ? null_elem[c] : 0ULL;
+    a.out[c] = (unsigned char*)cols_out[c];
+  }
+  // each segment's device alias (pinned host memory: the rows stay where they are)
+  std::vector<const unsigned char*> alias((size_t)ncols * nseg);
+  for (size_t k = 0; k < alias.size(); ++k) {
+    void* d = nullptr;
+    if (seg_rows[k % nseg + 1] > seg_rows[k % nseg]) {
+      if (!seg_ptrs[k]) return fail(PF_EINVAL, "gather_segments: a segment with rows is null");
+      cudaError_t e = cudaHostGetDevicePointer(&d, seg_ptrs[k], 0);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(PF_EINVAL, "gather_segments: a segment is not pinned host memory (%s)",
+                    cudaGetErrorString(e));
+      }
+    }
+    alias[k] = (const unsigned char*)d;
+  }
+  if (n == 0) return ok();
+  if (!idx) return fail(PF_EINVAL, "gather_segments: null index");
+  // pageable sources: the copies take the data before they return
+  PF_CUDA(cudaMemcpyAsync(dseg, alias.data(), alias.size() * sizeof(void*),
+                          cudaMemcpyHostToDevice, st));
+  PF_CUDA(cudaMemcpyAsync(drows, seg_rows, ((size_t)nseg + 1) * sizeof(long long),
+                          cudaMemcpyHostToDevice, st));
+  a.seg = dseg;
+  a.seg_rows = drows;
+  a.nseg = nseg;
+  a.ncols = ncols;
+  a.base = base;
+  a.idx = (const long long*)idx;
+  a.order = (const long long*)order;
+  a.n = n;
+  a.null_idx = null_idx;
+  a.allow_null = allow_null;
+  a.bad = (unsigned long long*)bad;
+  const unsigned g = (unsigned)std::max<long long>(
+      1, std::min<long long>((n + ZT - 1) / ZT, (long long)sm_count() * 8));
+  {
+    PF_KERNEL("k_gather_segments", st);
+    k_gather_segments<<<g, ZT, 0, st>>>(a);
+  }
+  PF_LAUNCH("k_gather_segments");
   return ok();
 }

@@ -869,11 +869,18 @@ static_assert(SJ_TS < 0xffff, "slots fit the 16-bit slot index");
 constexpr long long P2SEG = 16LL * P2TILE;
 
 // Rows a (sub-)bucket's region holds for `mean` expected rows: seven
-// standard deviations over the mean (the count is binomial, its deviation
-// below sqrt(mean)) and a few rows more.
-inline long long region_rows(double mean) {
-  return (long long)std::ceil(mean + 7.0 * std::sqrt(mean)) + 32;
+// standard deviations over the mean and a few rows more.  A side of distinct
+// keys (the build side) lands binomially, its deviation below sqrt(mean);
+// the probe side repeats keys (each build key is met m times on average), so
+// its bucket counts vary with the build keys' as well: var ~ mean * (1 + m).
+// Its regions allow var = 8 * mean, repeats up to about seven a key; skewed
+// keys past that overflow, and the pass is counted instead.
+constexpr double REGION_VAR_BUILD = 1.0;
+constexpr double REGION_VAR_PROBE = 8.0;
+inline long long region_rows(double mean, double var_factor) {
+  return (long long)std::ceil(mean + 7.0 * std::sqrt(var_factor * mean)) + 32;
 }
+inline double region_var(int side) { return side ? REGION_VAR_PROBE : REGION_VAR_BUILD; }
 
 struct SegArgs {
   const int2* seg;          // (partition, index in the partition)
@@ -1195,33 +1202,63 @@ struct SJArgs {
 #ifndef PF_SJ_SUM32
 #define PF_SJ_SUM32 1
 #endif
+// PF_SJ_LIMB: the low 32 bits as two 16-bit limbs, each added into a 32-bit
+// word without reading it back (no carry to resolve: a limb word takes fewer
+// than 2^16 adds when the sub-partition has fewer than 2^16 probe rows; the
+// kernel checks that), the high word only when nonzero.
+#ifndef PF_SJ_LIMB
+#define PF_SJ_LIMB 0
+#endif
 struct SJSum {
-#if PF_SJ_SUM32
+#if PF_SJ_LIMB
+  unsigned l0, l1, hi;
+#elif PF_SJ_SUM32
   unsigned lo, hi;
 #else
   unsigned long long v;
 #endif
 };
-__device__ __forceinline__ void sj_sum_add(SJSum& c, long long val) {
-#if PF_SJ_SUM32
+__device__ __forceinline__ void sj_sum_add(SJSum& c, long long val, bool careful) {
+#if PF_SJ_LIMB
+  const unsigned long long u = (unsigned long long)val;
+  if (careful) {  // 2^16 or more probe rows: the low word whole, its carry read back
+    const unsigned l = (unsigned)u, h = (unsigned)(u >> 32);
+    const unsigned old = atomicAdd(&c.l0, l);
+    const unsigned hc = h + (old + l < old ? 1u : 0u);
+    if (hc) atomicAdd(&c.hi, hc);
+    return;
+  }
+  atomicAdd(&c.l0, (unsigned)u & 0xffffu);
+  atomicAdd(&c.l1, ((unsigned)u >> 16) & 0xffffu);
+  if (const unsigned h = (unsigned)(u >> 32)) atomicAdd(&c.hi, h);
+#elif PF_SJ_SUM32
+  (void)careful;
   const unsigned l = (unsigned)(unsigned long long)val;
   const unsigned h = (unsigned)((unsigned long long)val >> 32);
   const unsigned old = atomicAdd(&c.lo, l);
   const unsigned hc = h + (old + l < old ? 1u : 0u);
   if (hc) atomicAdd(&c.hi, hc);  // zero for a value below 2^32 without a carry
 #else
+  (void)careful;
   atomicAdd(&c.v, (unsigned long long)val);
 #endif
 }
 __device__ __forceinline__ unsigned long long sj_sum_get(const SJSum& c) {
-#if PF_SJ_SUM32
+#if PF_SJ_LIMB
+  return (unsigned long long)c.l0 + ((unsigned long long)c.l1 << 16) +
+         ((unsigned long long)c.hi << 32);
+#elif PF_SJ_SUM32
   return ((unsigned long long)c.hi << 32) | c.lo;
 #else
   return c.v;
 #endif
 }
 __device__ __forceinline__ void sj_sum_clear(SJSum& c) {
-#if PF_SJ_SUM32
+#if PF_SJ_LIMB
+  c.l0 = 0;
+  c.l1 = 0;
+  c.hi = 0;
+#elif PF_SJ_SUM32
   c.lo = 0;
   c.hi = 0;
 #else
@@ -1229,10 +1266,20 @@ __device__ __forceinline__ void sj_sum_clear(SJSum& c) {
 #endif
 }
 
+// PF_SJ_RING > 0: each warp streams its probe rows through a ring of
+// PF_SJ_RING + 1 shared-memory slots filled by cp.async, PF_SJ_RING rounds
+// ahead of the one it looks up (more loads in flight than registers allow)
+#ifndef PF_SJ_RING
+#define PF_SJ_RING 0
+#endif
+constexpr int SJ_RING = PF_SJ_RING;
+constexpr int SJ_RSLOTS = SJ_RING + 1;
+
 struct SJSmem {
   long long key[SJ_TS];
   SJSum sum[SJ_TS];
   unsigned cnt[SJ_TS];
+  P2Row ring[SJ_RING ? SJT / 32 : 1][SJ_RING ? SJ_RSLOTS : 1][32];
   unsigned short slot_of[SJ_CAP];  // the slot of each build row of the chunk
   long long min_sum;               // the key hashing to INT64_MIN, kept apart
   unsigned min_cnt, min_goff;
@@ -1257,7 +1304,7 @@ __device__ __forceinline__ unsigned sj_next(unsigned t) {
 // One probe row against the chunk's table: its value and 1 into the cell of
 // the build row with its key.
 __device__ __forceinline__ void sj_probe(SJSmem& S, long long key, long long val, int logS,
-                                         unsigned& matched) {
+                                         unsigned& matched, bool careful) {
   if (key == SJ_EMPTY) {
     if (S.has_min) {
       atomicAdd((unsigned long long*)&S.min_sum, (unsigned long long)val);
@@ -1271,7 +1318,7 @@ __device__ __forceinline__ void sj_probe(SJSmem& S, long long key, long long val
     const long long x = S.key[t];
     if (x == SJ_EMPTY) return;
     if (x == key) {
-      sj_sum_add(S.sum[t], val);
+      sj_sum_add(S.sum[t], val, careful);
       atomicAdd(&S.cnt[t], 1u);
       ++matched;
       return;
@@ -1322,6 +1369,9 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
       __syncthreads();
       continue;
     }
+    // with 16-bit limbs, a sub-partition of 2^16 or more probe rows adds
+    // its low words whole (block-uniform)
+    const bool careful = PF_SJ_LIMB && p1 - p0 >= 65536;
     for (long long c0 = b0; c0 < b1; c0 += SJ_CAP) {
       const int nb = (int)min((long long)SJ_CAP, b1 - c0);
 #if PF_SJ_PIPE
@@ -1365,7 +1415,33 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
       }
       __syncthreads();
       // probe, SJ_U rows a thread a round
-#if PF_SJ_PIPE
+#if PF_SJ_RING
+      {
+        // rounds r = 0, 1, ...: row p0 + tid + r * SJT; round r's row sits
+        // in slot r % SJ_RSLOTS of this lane's column of the warp's ring.
+        // Round 0 came in with the build; rounds 1 .. SJ_RING - 1 go out
+        // now, and each round refills the slot the round before it used
+        P2Row* ring = &S.ring[tid >> 5][0][tid & 31];
+        const P2Row* src = a.prec + p0 + tid;
+        const long long nr = rem > 0 ? (rem + SJT - 1) / SJT : 0;
+        if (nr > 0) ring[0] = row[0];
+        for (int k = 1; k < SJ_RING; ++k) {
+          if (k < nr) cp_async16(&ring[k * 32], src + (long long)k * SJT);
+          asm volatile("cp.async.commit_group;" ::: "memory");
+        }
+        for (long long r = 0; r < nr; ++r) {
+          const long long f = r + SJ_RING;  // the round this one fetches
+          if (f < nr)
+            cp_async16(&ring[(int)(f % SJ_RSLOTS) * 32], src + f * SJT);
+          asm volatile("cp.async.commit_group;" ::: "memory");
+          // round r's copy was committed SJ_RING groups ago
+          asm volatile("cp.async.wait_group %0;" ::"n"(SJ_RING) : "memory");
+          const P2Row x = ring[(int)(r % SJ_RSLOTS) * 32];
+          sj_probe(S, x.k, x.v, a.logS, matched, careful);
+        }
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+      }
+#elif PF_SJ_PIPE
       // the next round's rows load while this round's are looked up
       {
         P2Row nrow[SJ_U];
@@ -1378,7 +1454,7 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
             nrow[u] = u * SJT < rn ? stream_ld_row(pr + u * SJT) : P2Row{0, 0};
 #pragma unroll
           for (int u = 0; u < SJ_U; ++u)
-            if (u * SJT < r) sj_probe(S, row[u].k, row[u].v, a.logS, matched);
+            if (u * SJT < r) sj_probe(S, row[u].k, row[u].v, a.logS, matched, careful);
 #pragma unroll
           for (int u = 0; u < SJ_U; ++u) row[u] = nrow[u];
         }
@@ -1393,7 +1469,7 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
         }
 #pragma unroll
         for (int u = 0; u < SJ_U; ++u)
-          if (i0 + u * SJT + tid < p1) sj_probe(S, row[u].k, row[u].v, a.logS, matched);
+          if (i0 + u * SJT + tid < p1) sj_probe(S, row[u].k, row[u].v, a.logS, matched, careful);
       }
 #endif
       __syncthreads();
@@ -1594,13 +1670,37 @@ __global__ void __launch_bounds__(SJF_T, PF_SJF_MINB) k_sjoin_fp(SJArgs a) {
   if (bad_group) atomicAdd(&a.stats[2], bad_group);
 }
 
-// PF_JOIN_PATH=rounds|smem picks the join path; read on every call (the
-// workspace size depends on it, so query and call must see the same value).
-int join_path_smem() {
-  const char* e = getenv("PF_JOIN_PATH");
-  if (e && std::string(e) == "rounds") return 0;
-  if (e && std::string(e) == "smem") return 1;
-  return PF_JOIN_PATH_DEFAULT;
+// The run-time choices of one call (pf_join_knobs with the defaults filled
+// in): the join path, the shared-memory join's table, the build rows a
+// sub-partition aims at, and whether the radix passes count first.  Without
+// knobs from the caller, PF_JOIN_PATH=rounds|smem, PF_SJ_FP=0|1,
+// PF_SJ_TARGET=<rows> and PF_COUNTED=0|1 override the defaults (sweeps and
+// tests); the workspace depends on them, so a query and its call must see
+// the same ones.
+struct Knobs {
+  int smem;          // 1: the shared-memory join, 0: the L2-round join
+  int table;         // shared-memory join: 0 hash slots, 1 fingerprinted slots
+  long long target;  // build rows a sub-partition aims at
+  int counted;       // 1: both radix passes count their rows first
+};
+
+Knobs resolve_knobs(const pf_join_knobs* k) {
+  Knobs r{PF_JOIN_PATH_DEFAULT, PF_SJ_FP_DEFAULT, SJ_TARGET, 0};
+  if (k) {
+    r.smem = k->path == 0 ? 1 : 0;
+    r.table = k->table ? 1 : 0;
+    if (k->sub_rows > 0) r.target = k->sub_rows;
+    r.counted = k->counted ? 1 : 0;
+    return r;
+  }
+  if (const char* e = getenv("PF_JOIN_PATH")) {
+    if (std::string(e) == "rounds") r.smem = 0;
+    if (std::string(e) == "smem") r.smem = 1;
+  }
+  if (const char* e = getenv("PF_SJ_FP")) r.table = e[0] == '1';
+  if (const char* e = getenv("PF_SJ_TARGET")) r.target = std::max(64LL, atoll(e));
+  if (const char* e = getenv("PF_COUNTED")) r.counted = e[0] == '1';
+  return r;
 }
 
 // The interleaved slab split into the caller's sum and count arrays.
@@ -1748,13 +1848,44 @@ struct JaLayout {
   unsigned long long* ovf;     // [2]: a region of the first / second pass overflowed
 };
 
-// Sub-partitions a partition splits into at most (a power of two), and the
-// table of the shared-memory path: never finer than SJ_TARGET build rows.
-long long max_subparts(long long nb) {
-  return std::min<long long>(P2BINS, (long long)pow2_at_least((uint64_t)(nb / SJ_TARGET + 1)));
+// Sub-partitions a partition splits into at most (a power of two): never
+// finer than `target` build rows.
+long long max_subparts(long long nb, long long target) {
+  return std::min<long long>(P2BINS, (long long)pow2_at_least((uint64_t)(nb / target + 1)));
 }
 
-JaLayout ja_layout(Arena& a, long long nb, long long np, int B, long long n_groups) {
+// The second radix pass's and the join's share of the workspace, for nparts
+// partitions of at most maxp[side] rows: regions for partitions that full,
+// the plan of the counted pass, the join's counter.
+void take_second_pass(Arena& a, JaLayout& l, long long nb, long long np, int nparts,
+                      const long long maxp[2], long long target) {
+  const long long rows[2] = {nb, np};
+  const long long b2 = max_subparts(std::max(maxp[0], nb / std::max(1, nparts)), target);
+  l.s_max = (long long)nparts * b2;
+  for (int side = 0; side < 2; ++side)
+    l.rows2[side] = std::max(std::max<long long>(rows[side], 1),
+                             l.s_max * region_rows((double)maxp[side] / b2, region_var(side)));
+  l.pkey2 = a.take<long long>((size_t)l.rows2[0]);
+  l.pgrp2 = a.take<int>((size_t)l.rows2[0]);
+  l.prec2 = a.take<P2Row>((size_t)l.rows2[1]);
+  l.pstart = a.take<long long>(4 * (size_t)nparts);
+  for (int side = 0; side < 2; ++side) {
+    l.tstart[side] = a.take<int>((size_t)nparts + 1);
+    l.nseg_max[side] = rows[side] / P2SEG + nparts + 1;
+    l.seg2[side] = a.take<int2>((size_t)l.nseg_max[side]);
+    l.pseg2[side] = a.take<int>((size_t)nparts + 1);
+    l.hist2[side] = a.take<int>((size_t)l.nseg_max[side] * P2BINS);
+  }
+  l.tot2 = a.take<long long>(2 * (size_t)l.s_max);
+  l.cur2 = a.take<unsigned long long>(2 * (size_t)l.s_max);
+  l.beg2 = a.take<unsigned long long>(2 * (size_t)l.s_max);
+  l.start2 = a.take<unsigned long long>(2 * ((size_t)l.s_max + 1));
+  l.scan2 = a.take<long long>(scan_scratch_elems(l.s_max));
+  l.sj_counter = a.take<unsigned long long>(1);
+}
+
+JaLayout ja_layout(Arena& a, long long nb, long long np, int B, long long n_groups,
+                   const Knobs& kn) {
   JaLayout l{};
   long long chunk;
   int nb_ch, np_ch;
@@ -1768,7 +1899,7 @@ JaLayout ja_layout(Arena& a, long long nb, long long np, int B, long long n_grou
   l.reg = a.take<long long>(2 * (size_t)B);
   l.slab = a.take<unsigned long long>(2 * (size_t)std::max<long long>(n_groups, 1));
   l.ovf = a.take<unsigned long long>(2);
-  if (!join_path_smem()) {
+  if (!kn.smem) {
     l.pkey = a.take<long long>(std::max<long long>(nb, 1));
     l.pgrp = a.take<int>(std::max<long long>(nb, 1));
     l.pfk = a.take<long long>(std::max<long long>(np, 1));
@@ -1785,34 +1916,13 @@ JaLayout ja_layout(Arena& a, long long nb, long long np, int B, long long n_grou
   // first pass: a region of cap1 rows a bucket (at least the side's rows)
   const long long rows[2] = {nb, np};
   for (int side = 0; side < 2; ++side)
-    l.cap1[side] = std::max((rows[side] + B - 1) / B, region_rows((double)rows[side] / B));
+    l.cap1[side] = std::max((rows[side] + B - 1) / B,
+                            region_rows((double)rows[side] / B, region_var(side)));
   l.pkey = a.take<long long>((size_t)B * l.cap1[0]);
   l.pgrp = a.take<int>((size_t)B * l.cap1[0]);
   l.prec = a.take<P2Row>((size_t)B * l.cap1[1]);
-  // second pass: regions for partitions as full as the first pass's regions
-  const long long b2 = max_subparts(nb);
-  l.s_max = (long long)B * b2;
-  for (int side = 0; side < 2; ++side)
-    l.rows2[side] = std::max(std::max<long long>(rows[side], 1),
-                             l.s_max * region_rows((double)l.cap1[side] / b2));
-  l.pkey2 = a.take<long long>((size_t)l.rows2[0]);
-  l.pgrp2 = a.take<int>((size_t)l.rows2[0]);
-  l.prec2 = a.take<P2Row>((size_t)l.rows2[1]);
-  l.pstart = a.take<long long>(4 * (size_t)B);
-  for (int side = 0; side < 2; ++side) {
-    l.tstart[side] = a.take<int>((size_t)B + 1);
-    l.nseg_max[side] = rows[side] / P2SEG + B + 1;
-    l.seg2[side] = a.take<int2>((size_t)l.nseg_max[side]);
-    l.pseg2[side] = a.take<int>((size_t)B + 1);
-    l.hist2[side] = a.take<int>((size_t)l.nseg_max[side] * P2BINS);
-  }
-  l.tot2 = a.take<long long>(2 * (size_t)l.s_max);
-  l.cur2 = a.take<unsigned long long>(2 * (size_t)l.s_max);
-  l.beg2 = a.take<unsigned long long>(2 * (size_t)l.s_max);
+  take_second_pass(a, l, nb, np, B, l.cap1, kn.target);
   l.cur1 = a.take<unsigned long long>(2 * (size_t)B);
-  l.start2 = a.take<unsigned long long>(2 * ((size_t)l.s_max + 1));
-  l.scan2 = a.take<long long>(scan_scratch_elems(l.s_max));
-  l.sj_counter = a.take<unsigned long long>(1);
   return l;
 }
 
@@ -1998,8 +2108,17 @@ int first_pass(const int64_t* build_key, const int32_t* build_group, long long n
 // contiguous; beg = start2, end = start2 + 1); else regions of cap2 rows
 // (beg = their starts, end = the cursors after the scatter; an overflow
 // raises ovf[1]).
-int second_pass(const JaLayout& l, int side, bool counted, long long cap2, int B, int logB2,
-                int logS, const long long* hcnt, const long long* d_pstart,
+// The first pass's output as the second pass reads it: build rows as (hash,
+// group) columns, probe rows as records, partition p of a side at the rows
+// the device array `part` gives (starts of both sides, then rows).
+struct P1View {
+  const long long* bkey;
+  const int* bgrp;
+  const P2Row* prec;
+};
+
+int second_pass(const JaLayout& l, const P1View& v, int side, bool counted, long long cap2,
+                int B, int logB2, int logS, const long long* hcnt, const long long* d_pstart,
                 const long long* d_pcnt, const unsigned long long** beg,
                 const unsigned long long** end, cudaStream_t st) {
   const long long S = (long long)B << logB2;
@@ -2027,8 +2146,8 @@ int second_pass(const JaLayout& l, int side, bool counted, long long cap2, int B
     if (g.nseg) {
       PF_KERNEL("k_p2_hist", st);
       const unsigned grid = (unsigned)std::min<long long>(g.nseg, sms * 4LL);
-      if (side) k_p2_hist<true><<<grid, P2T, 0, st>>>(nullptr, l.prec, g, l.hist2[side]);
-      else k_p2_hist<false><<<grid, P2T, 0, st>>>(l.pkey, nullptr, g, l.hist2[side]);
+      if (side) k_p2_hist<true><<<grid, P2T, 0, st>>>(nullptr, v.prec, g, l.hist2[side]);
+      else k_p2_hist<false><<<grid, P2T, 0, st>>>(v.bkey, nullptr, g, l.hist2[side]);
     }
     PF_LAUNCH("k_p2_hist");
     {
@@ -2077,52 +2196,56 @@ int second_pass(const JaLayout& l, int side, bool counted, long long cap2, int B
   a.ovf = l.ovf + 1;
   const size_t extra = ((size_t)B + 1) * sizeof(int);
   if (side) {
-    a.rec = l.prec;
+    a.rec = v.prec;
     a.rec_out = l.prec2;
     return p2_launch<0, true, P2BINS, P2I>(a, nt, extra, "k_p2_scatter", st);
   }
-  a.key = l.pkey;
-  a.val = l.pgrp;
+  a.key = v.bkey;
+  a.val = v.bgrp;
   a.key_out = l.pkey2;
   a.val_out = l.pgrp2;
   return p2_launch<0, false, P2BINS, P2I>(a, nt, extra, "k_p2_scatter", st);
 }
 
-// The shared-memory path after the first pass (counts on the host, hc[2B],
-// partitions at d_pstart): the second radix pass into sub-partitions of
-// about SJ_TARGET build rows, the join per sub-partition, the slab split.
-// A side whose regions would not fit its buffer, or every side after an
-// overflow, takes the counted second pass.  Keys are mix64 hashes here.
-int join_smem(const JaLayout& l, int B, int logB, const long long* hc, long long n_build,
-              long long n_probe, long long group_min, long long n_groups, int64_t* sum_out,
-              int64_t* count_out, int64_t* stats_out, long long* hstage, cudaStream_t st) {
-  (void)n_build;
-  (void)n_probe;
+// The shared-memory path after the first pass: the second radix pass of B
+// partitions (part: starts of both sides, then rows, on the host; logB the
+// bits of the hash the partitions share) into sub-partitions of about
+// kn.target build rows, the join per sub-partition into the slab (zeroed by
+// the caller), the slab split.  A side whose regions would not fit its
+// buffer, or every side after an overflow, takes the counted second pass.
+// Keys are mix64 hashes here.
+int join_smem(const JaLayout& l, const P1View& v, const Knobs& kn, int B, int logB,
+              const std::vector<long long>& part, long long group_min, long long n_groups,
+              int64_t* sum_out, int64_t* count_out, int64_t* stats_out, long long* hstage,
+              cudaStream_t st) {
+  // pageable source: the copy takes the data before it returns
+  PF_CUDA(cudaMemcpyAsync(l.pstart, part.data(), 4 * (size_t)B * sizeof(long long),
+                          cudaMemcpyHostToDevice, st));
+  const long long* hc = part.data() + 2 * (size_t)B;
   long long maxp[2] = {0, 0};
   for (int side = 0; side < 2; ++side)
     for (int p = 0; p < B; ++p) maxp[side] = std::max(maxp[side], hc[(size_t)side * B + p]);
   int logB2 = 0;
-  while ((maxp[0] >> logB2) > SJ_TARGET && logB2 < P2MAXLOG &&
+  while ((maxp[0] >> logB2) > kn.target && logB2 < P2MAXLOG &&
          ((long long)B << (logB2 + 1)) <= l.s_max)
     ++logB2;
   const int logS = logB + logB2;
   const long long S = 1LL << logS;
   const int sms = sm_count();
-  const char* force = getenv("PF_COUNTED");
   bool counted[2];
   long long cap2[2];
   for (int side = 0; side < 2; ++side) {
-    cap2[side] = region_rows((double)maxp[side] / (double)(1LL << logB2));
-    counted[side] = (force && force[0] == '1') || S * cap2[side] > l.rows2[side];
+    cap2[side] = region_rows((double)maxp[side] / (double)(1LL << logB2), region_var(side));
+    counted[side] = kn.counted || S * cap2[side] > l.rows2[side];
   }
   for (int attempt = 0; attempt < 2; ++attempt) {
     PF_CUDA(cudaMemsetAsync(l.ovf + 1, 0, sizeof(unsigned long long), st));
     const unsigned long long *bbeg, *bend, *pbeg, *pend;
-    if (int rc = second_pass(l, 0, counted[0], cap2[0], B, logB2, logS, hc, l.pstart,
+    if (int rc = second_pass(l, v, 0, counted[0], cap2[0], B, logB2, logS, hc, l.pstart,
                              l.pstart + 2 * B, &bbeg, &bend, st))
       return rc;
-    if (int rc = second_pass(l, 1, counted[1], cap2[1], B, logB2, logS, hc + B, l.pstart + B,
-                             l.pstart + 3 * B, &pbeg, &pend, st))
+    if (int rc = second_pass(l, v, 1, counted[1], cap2[1], B, logB2, logS, hc + B,
+                             l.pstart + B, l.pstart + 3 * B, &pbeg, &pend, st))
       return rc;
     SJArgs a{};
     a.bkey = l.pkey2;
@@ -2141,8 +2264,7 @@ int join_smem(const JaLayout& l, int B, int logB, const long long* hc, long long
     a.counter = l.sj_counter;
     a.ovf = l.ovf + 1;
     PF_CUDA(cudaMemsetAsync(l.sj_counter, 0, sizeof(unsigned long long), st));
-    const char* fpe = getenv("PF_SJ_FP");
-    if (fpe ? fpe[0] == '1' : PF_SJ_FP_DEFAULT) {
+    if (kn.table) {
       const size_t smem = sizeof(SJFSmem);
       if (int rc = opt_in_smem((const void*)k_sjoin_fp, smem)) return rc;
       int per_sm = 0;
@@ -2191,12 +2313,17 @@ extern "C" int pf_join_aggregate_pick_b(int64_t n_build, int64_t n_probe) {
 
 extern "C" int pf_join_aggregate_counted_passes(void) { return g_counted_passes; }
 
-extern "C" size_t pf_join_aggregate_workspace(int64_t n_build, int64_t n_probe, int B,
-                                              int64_t n_groups) {
+extern "C" size_t pf_join_aggregate_workspace_ex(int64_t n_build, int64_t n_probe, int B,
+                                                 int64_t n_groups, const pf_join_knobs* knobs) {
   if (B < 1) B = 1;
   Arena a(nullptr, 0);
-  ja_layout(a, n_build, n_probe, B, n_groups);
+  ja_layout(a, n_build, n_probe, B, n_groups, resolve_knobs(knobs));
   return a.used + 256;
+}
+
+extern "C" size_t pf_join_aggregate_workspace(int64_t n_build, int64_t n_probe, int B,
+                                              int64_t n_groups) {
+  return pf_join_aggregate_workspace_ex(n_build, n_probe, B, n_groups, nullptr);
 }
 
 extern "C" int pf_join_aggregate(const int64_t* build_key, const int32_t* build_group,
@@ -2206,7 +2333,23 @@ extern "C" int pf_join_aggregate(const int64_t* build_key, const int32_t* build_
                                  int64_t n_groups, int64_t* sum_out, int64_t* count_out,
                                  int64_t* stats_out, void* workspace, size_t workspace_bytes,
                                  void* stream) {
+  return pf_join_aggregate_ex(build_key, build_group, n_build, probe_fk, probe_price, probe_disc,
+                              scale, n_probe, B, group_min, n_groups, sum_out, count_out,
+                              stats_out, nullptr, workspace, workspace_bytes, stream);
+}
+
+extern "C" int pf_join_aggregate_ex(const int64_t* build_key, const int32_t* build_group,
+                                    int64_t n_build, const int64_t* probe_fk,
+                                    const int64_t* probe_price, const int64_t* probe_disc,
+                                    int64_t scale, int64_t n_probe, int B, int64_t group_min,
+                                    int64_t n_groups, int64_t* sum_out, int64_t* count_out,
+                                    int64_t* stats_out, const pf_join_knobs* knobs,
+                                    void* workspace, size_t workspace_bytes, void* stream) {
   cudaStream_t st = (cudaStream_t)stream;
+  const Knobs kn = resolve_knobs(knobs);
+  if (knobs && (knobs->path < 0 || knobs->path > 1 || knobs->sub_rows < 0))
+    return fail(PF_EINVAL, "join_aggregate: knobs path %d, sub_rows %d", knobs->path,
+                knobs->sub_rows);
   if (B < 1 || B > FB_MAX || (B & (B - 1)))
     return fail(PF_EINVAL, "join_aggregate: B must be a power of two in [1, %d], got %d", FB_MAX, B);
   if (n_build < 0 || n_probe < 0 || n_groups < 1 || n_groups > 0xfffffffeLL)
@@ -2215,7 +2358,7 @@ extern "C" int pf_join_aggregate(const int64_t* build_key, const int32_t* build_
   if (n_build >= (1LL << 40) || n_probe >= (1LL << 40))
     return fail(PF_EINVAL, "join_aggregate: at most 2^40 rows a side");
   Arena ar(workspace, workspace_bytes);
-  JaLayout l = ja_layout(ar, n_build, n_probe, B, n_groups);
+  JaLayout l = ja_layout(ar, n_build, n_probe, B, n_groups, kn);
   if (!workspace || !ar.fits())
     return fail(PF_ENOSPACE, "join_aggregate: workspace of %zu bytes, %zu needed",
                 workspace_bytes, ar.used);
@@ -2231,10 +2374,9 @@ extern "C" int pf_join_aggregate(const int64_t* build_key, const int32_t* build_
   long long* hc = pinned_counts(2 * (size_t)B + 8);
   if (!hc) return fail(PF_ECUDA, "join_aggregate: no pinned staging buffer");
   const int sms = sm_count();
-  if (join_path_smem()) {
+  if (kn.smem) {
     // 1: the first pass into regions of cap1 rows a bucket, from their starts
-    const char* force = getenv("PF_COUNTED");
-    bool counted = force && force[0] == '1';
+    bool counted = kn.counted != 0;
     std::vector<long long> part(4 * (size_t)B);  // starts, then rows, of both sides
     if (!counted) {
       for (int side = 0; side < 2; ++side) {
@@ -2284,11 +2426,8 @@ extern "C" int pf_join_aggregate(const int64_t* build_key, const int32_t* build_
       }
     }
     g_counted_passes = counted ? 1 : 0;
-    // pageable source: the copy takes the data before it returns
-    PF_CUDA(cudaMemcpyAsync(l.pstart, part.data(), part.size() * sizeof(long long),
-                            cudaMemcpyHostToDevice, st));
-    return join_smem(l, B, logB, part.data() + 2 * (size_t)B, n_build, n_probe, group_min,
-                     n_groups, sum_out, count_out, stats_out, hc, st);
+    return join_smem(l, P1View{l.pkey, l.pgrp, l.prec}, kn, B, logB, part, group_min, n_groups,
+                     sum_out, count_out, stats_out, hc, st);
   }
 
   // the round path: counts, then the first pass, queued while the host waits
@@ -2472,4 +2611,148 @@ extern "C" int pf_groups_finish(const int64_t* sum, const int64_t* count, int64_
   PF_LAUNCH("k_gemit");
   if (int rc = wait_event(ev)) return rc;
   return ok();
+}
+
+// ---- the join sharded over ranks: its two local phases ----------------------------
+//
+// Rank-local halves of pf_join_aggregate for a join whose rows are spread
+// over ranks: pf_join_partition hashes and radix-partitions a rank's rows
+// (counted, so every bucket is contiguous and the buckets can be sent to
+// their owners as they lie); after the exchange, pf_join_aggregate_buckets
+// runs the second radix pass and the join over the buckets a rank owns,
+// each bucket's rows contiguous, into a dense slab the ranks then add up.
+
+namespace pf {
+namespace {
+JaLayout partition_layout(Arena& a, long long nb, long long np, int B) {
+  JaLayout l{};
+  long long chunk;
+  int nb_ch, np_ch;
+  chunking(nb, &chunk, &nb_ch);
+  chunking(np, &chunk, &np_ch);
+  l.hist_b = a.take<int>((size_t)nb_ch * B);
+  l.hist_p = a.take<int>((size_t)np_ch * B);
+  l.cnt = a.take<long long>(2 * (size_t)B);
+  l.start = a.take<long long>(2 * (size_t)B);
+  l.total = a.take<long long>(2);
+  l.cur1 = a.take<unsigned long long>(2 * (size_t)B);
+  l.ovf = a.take<unsigned long long>(2);
+  return l;
+}
+
+JaLayout buckets_layout(Arena& a, const int64_t* counts, int nbk, long long n_groups,
+                        const Knobs& kn) {
+  JaLayout l{};
+  long long rows[2] = {0, 0}, maxp[2] = {0, 0};
+  for (int side = 0; side < 2; ++side)
+    for (int p = 0; p < nbk; ++p) {
+      rows[side] += counts[(size_t)side * nbk + p];
+      maxp[side] = std::max<long long>(maxp[side], counts[(size_t)side * nbk + p]);
+    }
+  l.slab = a.take<unsigned long long>(2 * (size_t)std::max<long long>(n_groups, 1));
+  l.ovf = a.take<unsigned long long>(2);
+  take_second_pass(a, l, rows[0], rows[1], nbk, maxp, kn.target);
+  return l;
+}
+}  // namespace
+}  // namespace pf
+
+extern "C" size_t pf_join_partition_workspace(int64_t n_build, int64_t n_probe, int B) {
+  if (B < 1) B = 1;
+  Arena a(nullptr, 0);
+  partition_layout(a, n_build, n_probe, B);
+  return a.used + 256;
+}
+
+extern "C" int pf_join_partition(const int64_t* build_key, const int32_t* build_group,
+                                 int64_t n_build, const int64_t* probe_fk,
+                                 const int64_t* probe_price, const int64_t* probe_disc,
+                                 int64_t scale, int64_t n_probe, int B, int64_t* build_hash_out,
+                                 int32_t* build_group_out, int64_t* probe_rec_out,
+                                 int64_t* host_counts, void* workspace, size_t workspace_bytes,
+                                 void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (B < 1 || B > FB_MAX || (B & (B - 1)))
+    return fail(PF_EINVAL, "join_partition: B must be a power of two in [1, %d], got %d", FB_MAX,
+                B);
+  if (n_build < 0 || n_probe < 0 || n_build >= (1LL << 40) || n_probe >= (1LL << 40))
+    return fail(PF_EINVAL, "join_partition: bad sizes (build %lld, probe %lld)",
+                (long long)n_build, (long long)n_probe);
+  if (!host_counts) return fail(PF_EINVAL, "join_partition: null host_counts");
+  Arena ar(workspace, workspace_bytes);
+  JaLayout l = partition_layout(ar, n_build, n_probe, B);
+  if (!workspace || !ar.fits())
+    return fail(PF_ENOSPACE, "join_partition: workspace of %zu bytes, %zu needed",
+                workspace_bytes, ar.used);
+  if (n_build == 0 && n_probe == 0) {
+    for (int i = 0; i < 2 * B; ++i) host_counts[i] = 0;
+    return ok();
+  }
+  l.pkey = (long long*)build_hash_out;
+  l.pgrp = build_group_out;
+  l.prec = (P2Row*)probe_rec_out;
+  const int logB = log2_exact((uint64_t)B);
+  cudaEvent_t ev;
+  if (int rc = count_buckets(build_key, n_build, probe_fk, n_probe, logB, B, l,
+                             (long long*)host_counts, &ev,
+                             st))
+    return rc;
+  PF_CUDA(cudaMemcpyAsync(l.cur1, l.start, 2 * B * sizeof(long long), cudaMemcpyDeviceToDevice,
+                          st));
+  const long long none[2] = {0, 0};
+  if (int rc = first_pass(build_key, build_group, n_build, probe_fk, probe_price, probe_disc,
+                          scale, n_probe, logB, B, none, l, st))
+    return rc;
+  return wait_event(ev);
+}
+
+extern "C" size_t pf_join_aggregate_buckets_workspace(const int64_t* counts, int nbk,
+                                                      int64_t n_groups,
+                                                      const pf_join_knobs* knobs) {
+  if (!counts || nbk < 1) return 256;
+  Arena a(nullptr, 0);
+  buckets_layout(a, counts, nbk, n_groups, resolve_knobs(knobs));
+  return a.used + 256;
+}
+
+extern "C" int pf_join_aggregate_buckets(const int64_t* build_hash, const int32_t* build_group,
+                                         const int64_t* probe_rec, const int64_t* counts,
+                                         int nbk, int logB, int64_t group_min, int64_t n_groups,
+                                         int64_t* sum_out, int64_t* count_out,
+                                         int64_t* stats_out, const pf_join_knobs* knobs,
+                                         void* workspace, size_t workspace_bytes, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  const Knobs kn = resolve_knobs(knobs);
+  if (!kn.smem) return fail(PF_EINVAL, "join_aggregate_buckets: the shared-memory join only");
+  if (!counts || nbk < 1 || logB < 0 || logB > 12 || nbk > (1 << logB))
+    return fail(PF_EINVAL, "join_aggregate_buckets: %d buckets of %d hash bits", nbk, logB);
+  if (n_groups < 1 || n_groups > 0xfffffffeLL)
+    return fail(PF_EINVAL, "join_aggregate_buckets: bad group count %lld", (long long)n_groups);
+  Arena ar(workspace, workspace_bytes);
+  JaLayout l = buckets_layout(ar, counts, nbk, n_groups, kn);
+  if (!workspace || !ar.fits())
+    return fail(PF_ENOSPACE, "join_aggregate_buckets: workspace of %zu bytes, %zu needed",
+                workspace_bytes, ar.used);
+  PF_CUDA(cudaMemsetAsync(stats_out, 0, 4 * sizeof(long long), st));
+  std::vector<long long> part(4 * (size_t)nbk);
+  long long tot[2] = {0, 0};
+  for (int side = 0; side < 2; ++side)
+    for (int p = 0; p < nbk; ++p) {
+      const size_t i = (size_t)side * nbk + p;
+      if (counts[i] < 0) return fail(PF_EINVAL, "join_aggregate_buckets: negative count");
+      part[i] = tot[side];
+      part[2 * (size_t)nbk + i] = counts[i];
+      tot[side] += counts[i];
+    }
+  if (tot[0] == 0 || tot[1] == 0) {
+    PF_CUDA(cudaMemsetAsync(sum_out, 0, n_groups * sizeof(long long), st));
+    PF_CUDA(cudaMemsetAsync(count_out, 0, n_groups * sizeof(long long), st));
+    return ok();
+  }
+  PF_CUDA(cudaMemsetAsync(l.slab, 0, 2 * n_groups * sizeof(unsigned long long), st));
+  long long* hc = pinned_counts(8);
+  if (!hc) return fail(PF_ECUDA, "join_aggregate_buckets: no pinned staging buffer");
+  return join_smem(l, P1View{(const long long*)build_hash, build_group, (const P2Row*)probe_rec},
+                   kn, nbk, logB, part, group_min, n_groups, sum_out, count_out, stats_out, hc,
+                   st);
 }

@@ -92,3 +92,62 @@ def index_select(x: torch.Tensor, idx: torch.Tensor) -> torch.Tensor:
 
 def index_with_null(x: torch.Tensor, idx: torch.Tensor) -> torch.Tensor:
     return _gather([x], idx, True)[0]
+
+
+def gather_from_host(segments: Sequence[Sequence[torch.Tensor]], seg_rows: Sequence[int],
+                     idx: torch.Tensor, allow_null: bool = True, base: int = 0,
+                     sorted_reads: bool = True) -> tuple:
+    """Zero-copy late materialization (pf_gather_segments): ``segments[c][s]``
+    is column c's segment s in pinned host memory, holding rows
+    ``[seg_rows[s], seg_rows[s + 1])``; returns each column's rows
+    ``idx + base`` on idx's device, read in place over the host link, a null
+    row (-64 as the dtype) where idx is -64, and the count of indexes outside
+    the segments (their rows are null too).  With ``sorted_reads`` the rows
+    are fetched in ascending index order, so neighbouring threads read
+    neighbouring host rows (the reference's zero_copy_rearrange argsorts its
+    indexes for the same reason, IO/zero_copy_reader.cu:84-90)."""
+    _native.require_cuda(idx, "gather index")
+    if idx.dtype != torch.int64 or idx.dim() != 1:
+        raise RuntimeError("gather index must be 1-D int64")
+    ncols, nseg = len(segments), len(seg_rows) - 1
+    if ncols < 1 or ncols > MAX_COLUMNS or nseg < 1:
+        raise RuntimeError("gather_from_host: 1-16 columns of at least one segment")
+    idx = idx.contiguous()
+    n = idx.numel()
+    dev = idx.device
+    outs, rb, eb, nb, ptrs = [], [], [], [], []
+    for col in segments:
+        if len(col) != nseg:
+            raise RuntimeError("gather_from_host: every column has one tensor a segment")
+        like = col[0]
+        for s, t in enumerate(col):
+            if t.device.type != "cpu" or not t.is_pinned() or not t.is_contiguous():
+                raise RuntimeError("gather_from_host: segments must be contiguous pinned "
+                                   "host tensors")
+            if t.shape[0] != seg_rows[s + 1] - seg_rows[s] or t.dtype != like.dtype \
+                    or t.shape[1:] != like.shape[1:]:
+                raise RuntimeError("gather_from_host: a segment's rows or type disagree")
+        width = 1
+        for d in like.shape[1:]:
+            width *= d
+        outs.append(torch.empty((n,) + tuple(like.shape[1:]), dtype=like.dtype, device=dev))
+        rb.append(max(1, width) * like.element_size())
+        eb.append(like.element_size())
+        nb.append(null_bits(like.dtype))
+        ptrs.extend(t.data_ptr() if t.numel() else None for t in col)
+    bad = torch.zeros(1, dtype=torch.int64, device=dev)
+    if n == 0:
+        return outs, 0
+    order = torch.argsort(idx) if sorted_reads else None
+    L = lib()
+    ws_bytes = L.pf_gather_segments_workspace(ncols, nseg)
+    ws = _native.workspace(ws_bytes, dev)
+    check(L.pf_gather_segments(arr(ctypes.c_void_p, ptrs), arr(ctypes.c_int64, list(seg_rows)),
+                               nseg, base, ncols, arr(ctypes.c_int, rb), arr(ctypes.c_int, eb),
+                               arr(ctypes.c_uint64, nb), ptr(idx),
+                               ptr(order) if order is not None else None, n,
+                               1 if allow_null else 0, NULL, arr(ctypes.c_void_p,
+                                                                 [ptr(o) for o in outs]),
+                               ptr(bad), ws.data_ptr(), ws_bytes, stream_of(dev)),
+          "gather_segments")
+    return outs, int(bad.item())

@@ -1,6 +1,9 @@
-"""The fused join -> group-by on sm_100a (pf_join_aggregate): radix partition
-of both sides, per-round L2-resident hash tables, probe rows aggregated
-straight into a dense group slab, then the occupied groups compacted.
+"""The fused join -> group-by on sm_100a (pf_join_aggregate_ex): two radix
+passes of both sides into sub-partitions, a shared-memory hash table per
+sub-partition, probe rows aggregated into their build row's cell and each
+build row flushed once into a dense group slab, then the occupied groups
+compacted.  The fan-out and the join's table are picked by the autotuner
+(pageflow_b200.autotune) unless given.
 
     keys, sums, counts = join_group_aggregate(build_key, build_group,
                                               probe_fk, price, disc)
@@ -13,12 +16,19 @@ uvm/aggregate.py), with exact int64 sums.
 """
 from __future__ import annotations
 
+import ctypes
+import os
 from dataclasses import dataclass
 from typing import Optional
 
 import torch
 
 from . import _native as N
+
+
+# Environment overrides of the knobs (for sweeps and tests); while one is set
+# the autotuner stays off.
+_OVERRIDES = ("PF_JOIN_PATH", "PF_SJ_FP", "PF_SJ_TARGET", "PF_COUNTED")
 
 
 @dataclass
@@ -35,16 +45,31 @@ class JoinAggregate:
     queued work can be timed or captured as is)."""
 
     def __init__(self, n_build: int, n_probe: int, group_min: int, n_groups: int,
-                 device, B: Optional[int] = None, scale: int = 100):
+                 device, B: Optional[int] = None, scale: int = 100,
+                 knobs: Optional[dict] = None, autotune: Optional[bool] = None):
+        """``B`` and ``knobs`` (pf_join_knobs fields: path, table, sub_rows,
+        counted) fix the launch configuration; with neither given (and no
+        PF_* override in the environment) the first ``aggregate`` call picks
+        B, table and sub_rows by timing candidates on its inputs (a cached
+        choice of the shape class is used as is); with autotune=False, B
+        comes from pf_join_aggregate_pick_b."""
         self.n_build, self.n_probe = int(n_build), int(n_probe)
         self.group_min, self.n_groups = int(group_min), int(n_groups)
         self.scale = int(scale)
         self.device = torch.device(device)
         L = N.lib()
+        self.knobs = None if knobs is None else N.JoinKnobs(**knobs)
+        if autotune is None:
+            # the environment's overrides (sweeps, tests) fix the configuration
+            autotune = B is None and knobs is None and not any(
+                os.environ.get(v) for v in _OVERRIDES)
+        self.autotune = bool(autotune)
+        self.tuning = None          # the autotuner's Result once it has run
         self.B = int(B) if B else int(L.pf_join_aggregate_pick_b(self.n_build, self.n_probe))
-        self.ws_bytes = int(L.pf_join_aggregate_workspace(self.n_build, self.n_probe, self.B,
-                                                          self.n_groups))
-        self.ws = N.workspace(self.ws_bytes, self.device)
+        self.ws = None
+        self.ws_bytes = 0
+        if not self.autotune:
+            self._reserve()
         self.sum = torch.empty(self.n_groups, dtype=torch.int64, device=self.device)
         self.count = torch.empty(self.n_groups, dtype=torch.int64, device=self.device)
         self.stats = torch.zeros(4, dtype=torch.int64, device=self.device)
@@ -55,9 +80,65 @@ class JoinAggregate:
         self.fin_ws = N.workspace(self.fin_bytes, self.device)
         self.host = torch.zeros(2, dtype=torch.int64, pin_memory=True)
 
+    def _ws_for(self, B, knobs) -> int:
+        return int(N.lib().pf_join_aggregate_workspace_ex(
+            self.n_build, self.n_probe, B, self.n_groups,
+            None if knobs is None else ctypes.byref(knobs)))
+
+    def _reserve(self, need: Optional[int] = None) -> None:
+        need = self._ws_for(self.B, self.knobs) if need is None else need
+        if self.ws is None or self.ws_bytes < need:
+            self.ws = None
+            self.ws = N.workspace(need, self.device)
+            self.ws_bytes = need
+
+    def _launch(self, B, knobs, args) -> None:
+        build_key, build_group, probe_fk, probe_price, probe_disc = args
+        L = N.lib()
+        with torch.cuda.device(self.device):
+            rc = L.pf_join_aggregate_ex(
+                build_key.data_ptr(), build_group.data_ptr(), self.n_build,
+                probe_fk.data_ptr(), probe_price.data_ptr(), N.ptr(probe_disc), self.scale,
+                self.n_probe, B, self.group_min, self.n_groups, self.sum.data_ptr(),
+                self.count.data_ptr(), self.stats.data_ptr(),
+                None if knobs is None else ctypes.byref(knobs), self.ws.data_ptr(),
+                self.ws_bytes, N.stream_of(self.device))
+        N.check(rc, "join_aggregate")
+
+    def _tune(self, args) -> None:
+        from . import autotune as T
+        key = T.shape_class(torch.cuda.get_device_name(self.device), self.n_build,
+                            self.n_probe, self.n_groups)
+
+        def knobs_of(c):
+            return N.JoinKnobs(path=0, table=c.table, sub_rows=c.sub_rows, counted=0)
+
+        def time_of(c):
+            kn = knobs_of(c)
+            self._reserve(self._ws_for(c.B, kn))
+            stream = torch.cuda.current_stream(self.device)
+            self._launch(c.B, kn, args)           # warm-up
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            reps = 2
+            e0.record(stream)
+            for _ in range(reps):
+                self._launch(c.B, kn, args)
+            e1.record(stream)
+            e1.synchronize()
+            return e0.elapsed_time(e1) / reps
+
+        self.tuning = T.tune(key, self.B, time_of)
+        c = self.tuning.choice
+        self.B = c.B
+        self.knobs = knobs_of(c)
+        self._reserve()
+        self.autotune = False
+
     def aggregate(self, build_key, build_group, probe_fk, probe_price, probe_disc=None):
         """Queues the join + dense aggregation into ``self.sum`` /
-        ``self.count`` (waits once, for the bucket counts)."""
+        ``self.count`` (waits for the first radix pass's bucket ends, and at
+        the end for the second pass's overflow word)."""
         for t, n, dt, name in ((build_key, self.n_build, torch.int64, "build_key"),
                                (build_group, self.n_build, torch.int32, "build_group"),
                                (probe_fk, self.n_probe, torch.int64, "probe_fk"),
@@ -69,15 +150,10 @@ class JoinAggregate:
                                            and probe_disc.numel() == self.n_probe
                                            and probe_disc.is_contiguous()):
             raise ValueError("probe_disc must match probe_fk")
-        L = N.lib()
-        with torch.cuda.device(self.device):
-            rc = L.pf_join_aggregate(
-                build_key.data_ptr(), build_group.data_ptr(), self.n_build,
-                probe_fk.data_ptr(), probe_price.data_ptr(), N.ptr(probe_disc), self.scale,
-                self.n_probe, self.B, self.group_min, self.n_groups, self.sum.data_ptr(),
-                self.count.data_ptr(), self.stats.data_ptr(), self.ws.data_ptr(),
-                self.ws_bytes, N.stream_of(self.device))
-        N.check(rc, "join_aggregate")
+        args = (build_key, build_group, probe_fk, probe_price, probe_disc)
+        if self.autotune:
+            self._tune(args)
+        self._launch(self.B, self.knobs, args)
 
     def finish(self):
         """The occupied groups, ascending: (keys, sums, counts)."""

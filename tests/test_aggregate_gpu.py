@@ -335,3 +335,71 @@ def test_uniform_keys_fill_the_regions_without_counting(join_path):
     plan = JoinAggregate(w.n_build, w.n_probe, 0, w.n_groups, "cuda", B=64)
     _assert_groups(plan.run(bkey, bgrp, fk, price, disc), want)
     assert {"rounds": 1, "smem": 0, "smem-counted": 3}[join_path] == _counted_passes()
+
+
+@pytest.mark.parametrize("knobs", [dict(path=0, table=1, sub_rows=0, counted=0),
+                                   dict(path=0, table=1, sub_rows=682, counted=0),
+                                   dict(path=0, table=0, sub_rows=300, counted=0),
+                                   dict(path=0, table=1, sub_rows=0, counted=1),
+                                   dict(path=1, table=0, sub_rows=0, counted=0)])
+def test_every_knob_setting_gives_the_oracles_groups(knobs):
+    """pf_join_aggregate_ex with the autotuner's knobs set by hand: the join's
+    table, the sub-partition size, counted passes and the round path all
+    give the same groups."""
+    w = datagen.scaled(datagen.SCALE, 1 / 400)   # 375K x 1.5M, 3750 groups
+    bkey, bgrp = datagen.gen_build(w, "cuda")
+    fk, price, disc = datagen.gen_probe(w, "cuda")
+    want = _oracle_groups(bkey, bgrp, fk, price, disc, 0, w.n_groups)
+    for B in (16, 128):
+        plan = JoinAggregate(w.n_build, w.n_probe, 0, w.n_groups, "cuda", B=B, knobs=knobs)
+        _assert_groups(plan.run(bkey, bgrp, fk, price, disc), want)
+        assert plan.read_stats().matched == want[3]
+
+
+def test_fingerprint_table_with_extreme_and_skewed_keys():
+    """The fingerprinted table reserves no hash as a free mark: the key whose
+    mix64 is 2^63 and INT64_MIN / INT64_MAX join like any other; skewed
+    probe keys take the counted passes."""
+    knobs = dict(path=0, table=1, sub_rows=0, counted=0)
+    I = np.iinfo(np.int64)
+    ks = _unmix64(1 << 63)
+    bkey = torch.tensor([I.min, I.max, 0, -1, 5, I.min + 1, ks], dtype=torch.int64).cuda()
+    bgrp = torch.tensor([0, 1, 2, 3, 4, 5, 6], dtype=torch.int32).cuda()
+    fk = torch.tensor([I.min, I.min, I.max, 7, -1, I.min + 1, 0, I.min, ks, ks, ks + 1],
+                      dtype=torch.int64).cuda()
+    price = torch.arange(1, 12, dtype=torch.int64).cuda() * 1000
+    disc = torch.zeros(11, dtype=torch.int64).cuda()
+    want = _oracle_groups(bkey, bgrp, fk, price, disc, 0, 7)
+    for B in (1, 4):
+        plan = JoinAggregate(7, 11, 0, 7, "cuda", B=B, knobs=knobs)
+        _assert_groups(plan.run(bkey, bgrp, fk, price, disc), want)
+    g = torch.Generator().manual_seed(22)
+    nb, np_ = 100_000, 1_000_000
+    bkey = torch.randperm(4 * nb, generator=g)[:nb].to(torch.int64) * 7919 - (1 << 41)
+    bgrp = torch.randint(0, 2_000, (nb,), generator=g, dtype=torch.int32)
+    ranks = torch.rand(np_, generator=g).pow(8).mul(nb).to(torch.int64).clamp_(max=nb - 1)
+    args = [t.cuda() for t in (bkey, bgrp, bkey[ranks], torch.randint(0, 1 << 30, (np_,),
+                                                                   generator=g),
+                               torch.randint(0, 11, (np_,), generator=g))]
+    want = _oracle_groups(*args, 0, 2_000)
+    plan = JoinAggregate(nb, np_, 0, 2_000, "cuda", B=32, knobs=knobs)
+    _assert_groups(plan.run(*args), want)
+
+
+def test_autotuned_plan_matches_the_oracle_and_caches_its_choice(tmp_path, monkeypatch):
+    monkeypatch.setenv("PAGEFLOW_TUNE_CACHE", str(tmp_path / "tune.json"))
+    for v in ("PF_JOIN_PATH", "PF_SJ_FP", "PF_SJ_TARGET", "PF_COUNTED"):
+        monkeypatch.delenv(v, raising=False)
+    w = datagen.scaled(datagen.SCALE, 1 / 200)   # 750K x 3M, 7500 groups
+    bkey, bgrp = datagen.gen_build(w, "cuda")
+    fk, price, disc = datagen.gen_probe(w, "cuda")
+    want = _oracle_groups(bkey, bgrp, fk, price, disc, 0, w.n_groups)
+    plan = JoinAggregate(w.n_build, w.n_probe, 0, w.n_groups, "cuda")
+    assert plan.autotune
+    _assert_groups(plan.run(bkey, bgrp, fk, price, disc), want)
+    t = plan.tuning
+    assert t is not None and not t.cached and len(t.times_ms) >= 5
+    assert plan.B == t.choice.B and all(v > 0 for v in t.times_ms.values())
+    again = JoinAggregate(w.n_build, w.n_probe, 0, w.n_groups, "cuda")
+    _assert_groups(again.run(bkey, bgrp, fk, price, disc), want)
+    assert again.tuning.cached and again.tuning.choice == t.choice

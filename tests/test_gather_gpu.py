@@ -73,3 +73,37 @@ def test_gather_counts_out_of_range_and_reads_nothing_outside():
     sl = src[1:]
     assert gather.index_select(sl, torch.tensor([0, 98], device="cuda")).cpu().tolist() == [1, 99]
     assert gather.index_select(src, torch.empty(0, dtype=torch.int64, device="cuda")).numel() == 0
+
+
+@pytest.mark.parametrize("sorted_reads", [False, True])
+def test_gather_from_pinned_host_segments(sorted_reads):
+    """Rows read in place from pinned host memory (three segments of uneven
+    size, one empty), per dtype and row width: equal to indexing the
+    concatenated column, null rows for the null index and for indexes
+    outside the segments (counted, never read)."""
+    g = torch.Generator().manual_seed(31)
+    sizes = [700, 0, 1301, 55]
+    rows = [0]
+    for s in sizes:
+        rows.append(rows[-1] + s)
+    base = 1000
+    full = [torch.randint(-(1 << 40), 1 << 40, (rows[-1],), generator=g),
+            torch.randint(-100, 100, (rows[-1], 3), generator=g).to(torch.int16),
+            torch.randn(rows[-1], generator=g, dtype=torch.float64),
+            torch.randint(0, 255, (rows[-1], 25), generator=g).to(torch.uint8)]
+    segs = [[c[a:b].contiguous().pin_memory() for a, b in zip(rows[:-1], rows[1:])]
+            for c in full]
+    seg_rows = [r + base for r in rows]
+    n = 5000
+    idx = torch.randint(0, rows[-1], (n,), generator=g)
+    idx[::9] = -64
+    idx[5] = rows[-1] + 3          # past the last segment
+    idx[6] = -5                    # before the first
+    outs, bad = gather.gather_from_host(segs, seg_rows, idx.cuda(), base=base,
+                                        sorted_reads=sorted_reads)
+    assert bad == 2
+    nul = (idx == -64) | (idx < 0) | (idx >= rows[-1])
+    for o, c in zip(outs, full):
+        want = c[idx.clamp(0, rows[-1] - 1)]
+        want[nul] = torch.full((1,), -64, dtype=c.dtype)
+        assert torch.equal(o.cpu(), want)

@@ -98,3 +98,32 @@ def test_static_scratch_refuses_sizes_past_its_limit():
     wb, wp = _with_workspace(b, p, 1)
     n = int(cnt.item())
     assert torch.equal(bi[:n].cpu(), wb) and torch.equal(pi[:n].cpu(), wp)
+
+
+def test_static_calls_allocate_no_device_memory():
+    """After one call has set the scratch up (and loaded the module's
+    kernels), further calls leave both torch's allocator and the device's
+    free memory exactly where they were: the join's scratch is the library's
+    fixed array, its outputs are the caller's."""
+    b, p = _inputs(21, 200_000, 400_000, 1)
+    npr = p[0].numel()
+    bi = torch.empty(npr, dtype=torch.int64, device="cuda")
+    pi = torch.empty(npr, dtype=torch.int64, device="cuda")
+    cnt = torch.empty(1, dtype=torch.int64, device="cuda")
+    _native.check(_static(b, p, 1, bi, pi, cnt), "join_unique_hash_static")
+    torch.cuda.synchronize()
+    torch_before = torch.cuda.memory_allocated()
+    free_before, _ = torch.cuda.mem_get_info()
+    for seed in (22, 23, 24):
+        b2, p2 = _inputs(seed, 200_000, 400_000, 1)
+        torch.cuda.synchronize()
+        torch_mid = torch.cuda.memory_allocated()
+        free_mid, _ = torch.cuda.mem_get_info()
+        for _ in range(3):
+            _native.check(_static(b2, p2, 1, bi, pi, cnt), "join_unique_hash_static")
+        torch.cuda.synchronize()
+        assert torch.cuda.memory_allocated() == torch_mid
+        assert torch.cuda.mem_get_info()[0] == free_mid
+        del b2, p2
+    assert torch.cuda.memory_allocated() == torch_before
+    assert free_before > 0
