@@ -445,6 +445,23 @@ int pf_merge_sorted_runs(const int64_t* run_keys, const void* const* run_vals, i
  */
 int64_t pf_page_encode(const void* values, int esize, int64_t n, void* out, int64_t capacity);
 /*
+ * Output-side encoding on the device: an int32/int64 column (values, device,
+ * esize 4 or 8) cut into npages pages, page p = rows [page_rows[p],
+ * page_rows[p + 1]) (host int64, at most 2^30 rows a page; e.g. the buckets
+ * of a partitioned output), each written as a PFC1 page into out (device,
+ * capacity bytes), byte for byte the page pf_page_encode writes for the same
+ * values.  page_offsets (host int64[npages + 1]) receives each page's byte
+ * offset and the total.  The device counterpart of the reference's
+ * compression of partitioned outputs (IO/codec/region_producer.py, layout
+ * IO/codec/batched_compress.py:27-59), with this library's format.  Waits
+ * once, for the page sizes; PF_ENOSPACE when the pages exceed capacity
+ * (nothing written).
+ */
+size_t pf_encode_pages_workspace(int npages);
+int pf_encode_pages(const void* values, int esize, const int64_t* page_rows, int npages,
+                    void* out, int64_t capacity, int64_t* page_offsets, void* workspace,
+                    size_t workspace_bytes, void* stream);
+/*
  * The paged benchmark's probe table generated and encoded on host threads:
  * n_rows rows of 6 columns (fk int64 with Zipf ranks from the given table over
  * n_build keys, date int32 sorted within 2^20-row runs in [8035, 10591],

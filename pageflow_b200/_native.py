@@ -99,6 +99,8 @@ _SIGS = {
     "pf_merge_sorted_runs_workspace": (_sz, [_i64]),
     "pf_merge_sorted_runs": (_int, [_vp, _vp, _i64, _vp, _vp, _i64, _int, _vp, _vp, _vp, _vp,
                                     _vp, _vp, ctypes.POINTER(_i64), _vp, _sz, _vp]),
+    "pf_encode_pages_workspace": (_sz, [_int]),
+    "pf_encode_pages": (_int, [_vp, _int, _vp, _int, _vp, _i64, _vp, _vp, _sz, _vp]),
     "pf_page_encode": (_i64, [_vp, _int, _i64, _vp, _i64]),
     "pf_paged_generate": (_int, [ctypes.c_uint64, _i64, _int, _i64, _vp, _vp, _int, _int,
                                  ctypes.POINTER(_vp), ctypes.POINTER(_i64)]),

@@ -1202,63 +1202,33 @@ struct SJArgs {
 #ifndef PF_SJ_SUM32
 #define PF_SJ_SUM32 1
 #endif
-// PF_SJ_LIMB: the low 32 bits as two 16-bit limbs, each added into a 32-bit
-// word without reading it back (no carry to resolve: a limb word takes fewer
-// than 2^16 adds when the sub-partition has fewer than 2^16 probe rows; the
-// kernel checks that), the high word only when nonzero.
-#ifndef PF_SJ_LIMB
-#define PF_SJ_LIMB 0
-#endif
 struct SJSum {
-#if PF_SJ_LIMB
-  unsigned l0, l1, hi;
-#elif PF_SJ_SUM32
+#if PF_SJ_SUM32
   unsigned lo, hi;
 #else
   unsigned long long v;
 #endif
 };
-__device__ __forceinline__ void sj_sum_add(SJSum& c, long long val, bool careful) {
-#if PF_SJ_LIMB
-  const unsigned long long u = (unsigned long long)val;
-  if (careful) {  // 2^16 or more probe rows: the low word whole, its carry read back
-    const unsigned l = (unsigned)u, h = (unsigned)(u >> 32);
-    const unsigned old = atomicAdd(&c.l0, l);
-    const unsigned hc = h + (old + l < old ? 1u : 0u);
-    if (hc) atomicAdd(&c.hi, hc);
-    return;
-  }
-  atomicAdd(&c.l0, (unsigned)u & 0xffffu);
-  atomicAdd(&c.l1, ((unsigned)u >> 16) & 0xffffu);
-  if (const unsigned h = (unsigned)(u >> 32)) atomicAdd(&c.hi, h);
-#elif PF_SJ_SUM32
-  (void)careful;
+__device__ __forceinline__ void sj_sum_add(SJSum& c, long long val) {
+#if PF_SJ_SUM32
   const unsigned l = (unsigned)(unsigned long long)val;
   const unsigned h = (unsigned)((unsigned long long)val >> 32);
   const unsigned old = atomicAdd(&c.lo, l);
   const unsigned hc = h + (old + l < old ? 1u : 0u);
   if (hc) atomicAdd(&c.hi, hc);  // zero for a value below 2^32 without a carry
 #else
-  (void)careful;
   atomicAdd(&c.v, (unsigned long long)val);
 #endif
 }
 __device__ __forceinline__ unsigned long long sj_sum_get(const SJSum& c) {
-#if PF_SJ_LIMB
-  return (unsigned long long)c.l0 + ((unsigned long long)c.l1 << 16) +
-         ((unsigned long long)c.hi << 32);
-#elif PF_SJ_SUM32
+#if PF_SJ_SUM32
   return ((unsigned long long)c.hi << 32) | c.lo;
 #else
   return c.v;
 #endif
 }
 __device__ __forceinline__ void sj_sum_clear(SJSum& c) {
-#if PF_SJ_LIMB
-  c.l0 = 0;
-  c.l1 = 0;
-  c.hi = 0;
-#elif PF_SJ_SUM32
+#if PF_SJ_SUM32
   c.lo = 0;
   c.hi = 0;
 #else
@@ -1266,20 +1236,10 @@ __device__ __forceinline__ void sj_sum_clear(SJSum& c) {
 #endif
 }
 
-// PF_SJ_RING > 0: each warp streams its probe rows through a ring of
-// PF_SJ_RING + 1 shared-memory slots filled by cp.async, PF_SJ_RING rounds
-// ahead of the one it looks up (more loads in flight than registers allow)
-#ifndef PF_SJ_RING
-#define PF_SJ_RING 0
-#endif
-constexpr int SJ_RING = PF_SJ_RING;
-constexpr int SJ_RSLOTS = SJ_RING + 1;
-
 struct SJSmem {
   long long key[SJ_TS];
   SJSum sum[SJ_TS];
   unsigned cnt[SJ_TS];
-  P2Row ring[SJ_RING ? SJT / 32 : 1][SJ_RING ? SJ_RSLOTS : 1][32];
   unsigned short slot_of[SJ_CAP];  // the slot of each build row of the chunk
   long long min_sum;               // the key hashing to INT64_MIN, kept apart
   unsigned min_cnt, min_goff;
@@ -1304,7 +1264,7 @@ __device__ __forceinline__ unsigned sj_next(unsigned t) {
 // One probe row against the chunk's table: its value and 1 into the cell of
 // the build row with its key.
 __device__ __forceinline__ void sj_probe(SJSmem& S, long long key, long long val, int logS,
-                                         unsigned& matched, bool careful) {
+                                         unsigned& matched) {
   if (key == SJ_EMPTY) {
     if (S.has_min) {
       atomicAdd((unsigned long long*)&S.min_sum, (unsigned long long)val);
@@ -1318,7 +1278,7 @@ __device__ __forceinline__ void sj_probe(SJSmem& S, long long key, long long val
     const long long x = S.key[t];
     if (x == SJ_EMPTY) return;
     if (x == key) {
-      sj_sum_add(S.sum[t], val, careful);
+      sj_sum_add(S.sum[t], val);
       atomicAdd(&S.cnt[t], 1u);
       ++matched;
       return;
@@ -1369,9 +1329,6 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
       __syncthreads();
       continue;
     }
-    // with 16-bit limbs, a sub-partition of 2^16 or more probe rows adds
-    // its low words whole (block-uniform)
-    const bool careful = PF_SJ_LIMB && p1 - p0 >= 65536;
     for (long long c0 = b0; c0 < b1; c0 += SJ_CAP) {
       const int nb = (int)min((long long)SJ_CAP, b1 - c0);
 #if PF_SJ_PIPE
@@ -1415,33 +1372,7 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
       }
       __syncthreads();
       // probe, SJ_U rows a thread a round
-#if PF_SJ_RING
-      {
-        // rounds r = 0, 1, ...: row p0 + tid + r * SJT; round r's row sits
-        // in slot r % SJ_RSLOTS of this lane's column of the warp's ring.
-        // Round 0 came in with the build; rounds 1 .. SJ_RING - 1 go out
-        // now, and each round refills the slot the round before it used
-        P2Row* ring = &S.ring[tid >> 5][0][tid & 31];
-        const P2Row* src = a.prec + p0 + tid;
-        const long long nr = rem > 0 ? (rem + SJT - 1) / SJT : 0;
-        if (nr > 0) ring[0] = row[0];
-        for (int k = 1; k < SJ_RING; ++k) {
-          if (k < nr) cp_async16(&ring[k * 32], src + (long long)k * SJT);
-          asm volatile("cp.async.commit_group;" ::: "memory");
-        }
-        for (long long r = 0; r < nr; ++r) {
-          const long long f = r + SJ_RING;  // the round this one fetches
-          if (f < nr)
-            cp_async16(&ring[(int)(f % SJ_RSLOTS) * 32], src + f * SJT);
-          asm volatile("cp.async.commit_group;" ::: "memory");
-          // round r's copy was committed SJ_RING groups ago
-          asm volatile("cp.async.wait_group %0;" ::"n"(SJ_RING) : "memory");
-          const P2Row x = ring[(int)(r % SJ_RSLOTS) * 32];
-          sj_probe(S, x.k, x.v, a.logS, matched, careful);
-        }
-        asm volatile("cp.async.wait_group 0;" ::: "memory");
-      }
-#elif PF_SJ_PIPE
+#if PF_SJ_PIPE
       // the next round's rows load while this round's are looked up
       {
         P2Row nrow[SJ_U];
@@ -1454,7 +1385,7 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
             nrow[u] = u * SJT < rn ? stream_ld_row(pr + u * SJT) : P2Row{0, 0};
 #pragma unroll
           for (int u = 0; u < SJ_U; ++u)
-            if (u * SJT < r) sj_probe(S, row[u].k, row[u].v, a.logS, matched, careful);
+            if (u * SJT < r) sj_probe(S, row[u].k, row[u].v, a.logS, matched);
 #pragma unroll
           for (int u = 0; u < SJ_U; ++u) row[u] = nrow[u];
         }
@@ -1469,7 +1400,7 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
         }
 #pragma unroll
         for (int u = 0; u < SJ_U; ++u)
-          if (i0 + u * SJT + tid < p1) sj_probe(S, row[u].k, row[u].v, a.logS, matched, careful);
+          if (i0 + u * SJT + tid < p1) sj_probe(S, row[u].k, row[u].v, a.logS, matched);
       }
 #endif
       __syncthreads();

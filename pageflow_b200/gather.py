@@ -121,7 +121,8 @@ def gather_from_host(segments: Sequence[Sequence[torch.Tensor]], seg_rows: Seque
             raise RuntimeError("gather_from_host: every column has one tensor a segment")
         like = col[0]
         for s, t in enumerate(col):
-            if t.device.type != "cpu" or not t.is_pinned() or not t.is_contiguous():
+            if t.device.type != "cpu" or not t.is_contiguous() or (t.numel() and
+                                                                  not t.is_pinned()):
                 raise RuntimeError("gather_from_host: segments must be contiguous pinned "
                                    "host tensors")
             if t.shape[0] != seg_rows[s + 1] - seg_rows[s] or t.dtype != like.dtype \

@@ -68,6 +68,40 @@ def encode_page(values: np.ndarray) -> np.ndarray:
     return out[:n]
 
 
+def page_capacity(rows: int, esize: int) -> int:
+    """Bytes a PFC1 page of `rows` values takes at most (RAW, or a stream of
+    64-bit fields, whichever the encoder picks is never larger than both)."""
+    blocks = (rows + 1023) // 1024
+    return 64 + 16 + 32 * blocks + 8 * rows + 16 + 64
+
+
+def encode_pages_device(values: torch.Tensor, page_rows) -> tuple:
+    """Output-side encoding on the GPU (pf_encode_pages): ``values`` (a 1-D
+    int32 / int64 CUDA tensor) cut at ``page_rows`` (ascending, from 0 to
+    its length) into PFC1 pages, the same bytes pf_page_encode writes.
+    Returns (the pages, a uint8 CUDA tensor, and each page's byte offset
+    with the total)."""
+    _native.require_cuda(values, "encode_pages values")
+    if values.dtype not in (torch.int32, torch.int64) or values.dim() != 1:
+        raise TypeError("encode_pages: a 1-D int32 or int64 tensor")
+    values = values.contiguous()
+    rows = [int(r) for r in page_rows]
+    npages = len(rows) - 1
+    if npages < 1 or rows[0] != 0 or rows[-1] != values.numel():
+        raise ValueError("encode_pages: page rows run from 0 to the column's length")
+    es = values.element_size()
+    cap = sum(page_capacity(b - a, es) for a, b in zip(rows[:-1], rows[1:]))
+    out = torch.empty(cap, dtype=torch.uint8, device=values.device)
+    offs = (ctypes.c_int64 * (npages + 1))()
+    L = lib()
+    ws_bytes = L.pf_encode_pages_workspace(npages)
+    ws = _native.workspace(ws_bytes, values.device)
+    check(L.pf_encode_pages(ptr(values), es, arr(ctypes.c_int64, rows), npages, ptr(out), cap,
+                            offs, ptr(ws), ws_bytes, stream_of(values.device)), "encode_pages")
+    offsets = list(offs)
+    return out[:offsets[-1]], offsets
+
+
 class PagedTable:
     """A table as PFC1 pages in pinned host memory: row group g holds every
     column's page of rows [g * rows_per_page, (g + 1) * rows_per_page), in

@@ -109,3 +109,93 @@ def test_bad_page_is_counted_and_dropped():
     assert s["bad_pages"] == 4                              # the group's 4 CTAs
     assert s["rows"] == 2 * 16384
     assert parts.bucket_offsets.cpu().numpy()[1, 8] == 0
+
+
+# ---- output-side encoding on the device --------------------------------------------
+
+def _host_pages(values: np.ndarray, rows):
+    return [paged.encode_page(values[a:b]) for a, b in zip(rows[:-1], rows[1:])]
+
+
+def _encode_and_compare(kind):
+    """Every page the device encoder writes is byte for byte the host
+    encoder's page of the same values (so the same scheme is chosen), and
+    the oracle's decoder gives the values back; returns the schemes seen."""
+    rng = np.random.default_rng(sum(map(ord, kind)))
+    n = 300_000
+    if kind == "sorted_runs":        # DELTA / FOR: dates sorted within runs
+        v = (8035 + (np.arange(n) % 70_000) * 2557 // 70_000).astype(np.int32)
+    elif kind == "random_small":     # FOR
+        v = rng.integers(1, 50, n).astype(np.int64)
+    elif kind == "random_wide":      # RAW
+        v = rng.integers(-(1 << 62), 1 << 62, n).astype(np.int64)
+    elif kind == "constant":         # RLE, one run a page
+        v = np.full(n, 12345, np.int64)
+    elif kind == "few_runs":         # RLE with thousands of runs, and one page over its limit
+        v = np.repeat(rng.integers(0, 1 << 40, 6000), 50).astype(np.int64)
+    elif kind == "int32_negative":
+        v = rng.integers(-(1 << 31), 1 << 31, n).astype(np.int32) // 3
+    elif kind == "extremes":
+        v = rng.choice(np.array([np.iinfo(np.int64).min, np.iinfo(np.int64).max, 0, -1]),
+                       n).astype(np.int64)
+    else:
+        v = rng.integers(0, 1000, 5001).astype(np.int64)
+    n = v.shape[0]
+    cuts = sorted({0, n, *rng.integers(0, n, 5).tolist(), min(n, 1024), min(n, 1)})
+    if kind == "few_runs":
+        cuts = [0, 50 * 4000, n]         # 4000 runs, then 2000
+    if kind == "ragged":
+        cuts = [0, 0, 1, 1025, 1025, 2048, n]   # empty and one-value pages
+    got, offs = paged.encode_pages_device(torch.from_numpy(v).cuda(), cuts)
+    got = got.cpu().numpy()
+    want = _host_pages(v, cuts)
+    schemes = set()
+    for p, w in enumerate(want):
+        page = got[offs[p]:offs[p + 1]]
+        assert page.shape == w.shape and np.array_equal(page, w), f"page {p}"
+        schemes.add(int(page[4]))
+        dec = oracle.page_decode(page)
+        assert np.array_equal(dec.astype(v.dtype), v[cuts[p]:cuts[p + 1]])
+    assert offs[-1] == sum(w.shape[0] for w in want)
+    return schemes
+
+
+@pytest.mark.parametrize("kind", ["sorted_runs", "random_small", "random_wide", "constant",
+                                  "few_runs", "int32_negative", "extremes", "ragged"])
+def test_device_encoder_writes_the_host_encoders_bytes(kind):
+    _encode_and_compare(kind)
+
+
+def test_device_encoder_takes_every_scheme():
+    seen = set()
+    for kind in ("sorted_runs", "random_small", "random_wide", "constant"):
+        seen |= _encode_and_compare(kind)
+    assert seen == {0, 1, 2, 3}
+
+
+def test_partitioned_output_encoded_bucket_by_bucket():
+    """A partitioned column (the drop-in partition's padded layout) encoded
+    a bucket a page: each bucket's page decodes to its rows."""
+    from pageflow_b200 import tqpkernels
+    from tests.dropin import padded_starts
+    rng = np.random.default_rng(3)
+    n, B = 200_000, 16
+    key = torch.from_numpy(rng.integers(-(1 << 40), 1 << 40, n)).cuda()
+    qty = torch.from_numpy(rng.integers(1, 51, n).astype(np.int64)).cuda()
+    host = torch.empty(B + 5, dtype=torch.int64, pin_memory=True)
+    outs = tqpkernels.partition_sort([key, qty], [0, 0], 0, None, n, 0, B, False, host)
+    counts = host[:B].tolist()
+    starts, _ = padded_starts(counts, 8)
+    rows = []
+    for s0, c in zip(starts, counts):
+        rows += [s0, s0 + c]
+    # pages over the buckets' rows only (the padding between them is a page
+    # of its own, skipped)
+    cuts = sorted(set([0] + rows + [outs[1].numel()]))
+    pages, offs = paged.encode_pages_device(outs[1], cuts)
+    pages = pages.cpu().numpy()
+    col = outs[1].cpu().numpy()
+    for s0, c in zip(starts, counts):
+        p = cuts.index(s0)
+        assert cuts[p + 1] == s0 + c
+        assert np.array_equal(oracle.page_decode(pages[offs[p]:offs[p + 1]]), col[s0:s0 + c])
