@@ -48,6 +48,10 @@ def parse_args(argv=None):
     ap.add_argument("--workload", default="scale",
                     help="scale (150M x 600M), small (250K x 1M) or scale/<divisor>")
     ap.add_argument("--B", type=int, default=0, help="fan-out (0: the autotuner's pick)")
+    ap.add_argument("--parallelism", choices=["sharded", "replicas"], default=None,
+                    help="one join sharded over the ranks (each holds a slice of both sides; "
+                         "buckets move to their owners; the default for N > 1) or independent "
+                         "replicas (the default for N = 1)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -411,6 +415,100 @@ def run_ours(args, w, world, rank, local_rank):
             "kernels": kernels,
             "e2e": e2e, "cpu_baseline": cpu, "plain_form": plain, "clocks": clocks,
             "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def run_sharded(args, w, world, rank, local_rank):
+    """N > 1: one join over the ranks (weak scaling: every rank holds the
+    scale workload's rows, so the job joins N x 150M build rows with N x 600M
+    probe rows, keys permuted over all N x 150M).  A step: each rank
+    partitions its rows (pf_join_partition), sends every bucket to its owner
+    over NCCL point-to-point messages, joins the buckets it owns
+    (pf_join_aggregate_buckets) and the ranks add their group slabs (an
+    int64 all-reduce).  Device time, max over ranks."""
+    import dataclasses
+
+    import torch
+    import torch.distributed as dist
+
+    from pageflow_b200 import _native, datagen
+    from pageflow_b200.sharded import CudaPhases, ShardedJoinAggregate, dense_groups
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    g = dataclasses.replace(w, n_build=w.n_build * world, n_probe=w.n_probe * world)
+    bkey, bgrp = datagen.gen_build(g, dev, lo=rank * w.n_build, rows=w.n_build)
+    fk, price, disc = datagen.gen_probe(g, dev, lo=rank * w.n_probe, rows=w.n_probe)
+    B = args.B or max(256, world)
+    job = ShardedJoinAggregate(0, w.n_groups, B, scale=w.scale, phases=CudaPhases(dev))
+    for _ in range(args.warmup):
+        job.run(bkey, bgrp, fk, price, disc)
+    sums, counts = job.run(bkey, bgrp, fk, price, disc)
+    keys, _, _ = dense_groups(sums, counts, 0)
+    groups_out, matched = int(keys.numel()), int(counts.sum())
+    sampler = ClockSampler(None)
+    dist.barrier()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    launches0 = _native.launch_count()
+    e0.record(stream)
+    for _ in range(args.steps):
+        job.run(bkey, bgrp, fk, price, disc)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = _native.launch_count() - launches0
+    dist.barrier()
+    clocks = sampler.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1), world, dev)
+    rows_step = w.n_build + w.n_probe
+    value = job_rate(rows_step * args.steps, ms, world)
+    # end to end: every rank's inputs from pinned host memory each step, the
+    # dense groups back to the host
+    e2e = None
+    if not args.no_e2e:
+        host = [t.cpu().pin_memory() for t in (bkey, bgrp, fk, price, disc)]
+        dev_in = [bkey, bgrp, fk, price, disc]
+        h2d = sum(t.numel() * t.element_size() for t in host)
+
+        def e2e_step():
+            for d, h in zip(dev_in, host):
+                d.copy_(h, non_blocking=True)
+            su, co = job.run(*dev_in)
+            out = [su.to("cpu", non_blocking=True), co.to("cpu", non_blocking=True)]
+            return out, su.numel() * 16
+        e2e_step()
+        torch.cuda.synchronize()
+        dist.barrier()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        d2h = 0
+        for _ in range(args.e2e_steps):
+            _, d2h = e2e_step()
+        f1.record(stream)
+        torch.cuda.synchronize()
+        ems = max_over_ranks(f0.elapsed_time(f1), world, dev)
+        e2e = {"value": job_rate(rows_step * args.e2e_steps, ems, world), "unit": "rows/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": ems / args.e2e_steps}
+    moved = sum_over_ranks(sum(job.last["received_rows"]) - sum(job.last["kept_rows"]),
+                           world, dev)
+    if rank == 0:
+        line = {
+            "metric": "join+agg rows/s", "value": value, "unit": "rows/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int64", "data": "synthetic (seeded generator, inputs on the device)",
+            "config": {"workload": w.name + f" x{world} (sharded)",
+                       "build_rows": w.n_build * world, "probe_rows": w.n_probe * world,
+                       "groups": w.n_groups, "fanout_B": B, "parallelism": f"sharded{world}",
+                       "l2": "inputs exceed L2; no flush", "groups_out": groups_out,
+                       "matched_probe_rows": matched,
+                       "rows_moved_per_step": int(moved)},
+            "e2e": e2e, "clocks": clocks, "gpu_launches": launches,
         }
         print(json.dumps(line), flush=True)
 
@@ -1157,21 +1255,30 @@ def main(argv=None) -> int:
     run = {"batch": run_batch, "serve": run_serve, "paged": run_paged,
            "kernels": run_kernels}.get(mode)
     w = None if run else workload(args.workload)
-    if world > 1:
+    sharded = not run and (args.parallelism == "sharded" or
+                           (args.parallelism is None and world > 1))
+    if world > 1 or sharded:
         import datetime
 
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
+        if world == 1:   # a one-rank group of this process (no launcher)
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            os.environ.setdefault("MASTER_PORT", "29571")
+            os.environ.setdefault("RANK", "0")
+            os.environ.setdefault("WORLD_SIZE", "1")
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
     try:
         if run:
             run(args, world, rank, local_rank)
+        elif sharded:
+            run_sharded(args, w, world, rank, local_rank)
         else:
             run_ours(args, w, world, rank, local_rank)
     finally:
-        if world > 1:
+        if world > 1 or sharded:
             import torch.distributed as dist
             dist.destroy_process_group()
     return 0

@@ -935,7 +935,8 @@ __global__ void __launch_bounds__(P2T) k_p2_hist(const long long* __restrict__ k
 #pragma unroll
       for (int q = 0; q < P2I; ++q)
         if (t0 + q * P2T + tid < hi)
-          atomicAdd(&bins[bucket_of_hash((uint64_t)kk[q], g.logS) - base], 1);
+          atomicAdd(&bins[g.logB2 ? (int)(((uint64_t)kk[q] >> (64 - g.logS)) & (nb2 - 1)) : 0],
+                    1);
     }
     __syncthreads();
     for (int b = tid; b < nb2; b += P2T) hist[(long long)sg * nb2 + b] = bins[b];
@@ -2161,7 +2162,9 @@ int join_smem(const JaLayout& l, const P1View& v, const Knobs& kn, int B, int lo
          ((long long)B << (logB2 + 1)) <= l.s_max)
     ++logB2;
   const int logS = logB + logB2;
-  const long long S = 1LL << logS;
+  // sub-partitions: each of the B partitions split 2^logB2 ways (B need
+  // not be 2^logB: a rank of a sharded join holds some of the buckets)
+  const long long S = (long long)B << logB2;
   const int sms = sm_count();
   bool counted[2];
   long long cap2[2];

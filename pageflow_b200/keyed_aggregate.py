@@ -14,8 +14,11 @@ One chunk's rows are reduced to one row per group:
   buckets   with B > 1, each group's bucket (``_bucket_ids``) and the groups
             per bucket, on the host and on the device (pf_hash_buckets)
 
-Aggregates: ``('sum', col)``, ``('count', None)``, ``('min', col)``,
-``('max', col)`` and ``('avg', col)`` (its state: [sum, count]).  SUM of an
+Aggregates: ``('sum', col)``, ``('count', None)`` (every row) or
+``('count', col)`` (the rows whose value is not the null -64), ``('min',
+col)``, ``('max', col)`` (folded from 0, as the reference's partial is) and
+``('avg', col)`` (its state: [sum of every row, count of the non-null
+ones]), each as the reference's pass 1 computes it.  SUM of an
 integer column is exact in int64 (the reference sums through a float64
 bincount, :395-398, which equals it while every partial stays below 2^53).
 """
@@ -31,6 +34,7 @@ from . import _native
 from ._native import check, lib, ptr, stream_of
 from .sorted_run_merge import reduce_tick_slice
 
+NULL = -64   # the reference's null value (constants.null)
 COEFF_BASE_SEED = int(os.environ.get('TQP_HASH_SEED', '2029')) & 0x7FFF_FFFF_FFFF_FFFF
 
 
@@ -129,14 +133,21 @@ class KeyedPass1:
         n = h.numel()
         for op, cid in self.aggs:
             if op == 'count':
-                vals.append(torch.ones(n, dtype=torch.int64, device=h.device))
+                # COUNT(x) counts the rows whose x is not the null value
+                # (operator_utils.py:384-385); COUNT(*) every row
+                if cid is None:
+                    vals.append(torch.ones(n, dtype=torch.int64, device=h.device))
+                else:
+                    vals.append((columns[cid] != NULL).to(torch.int64))
                 ops.append('sum')
                 post.append(('count', len(vals) - 1))
             elif op == 'avg':
+                # the state [SUM(x), COUNT(x)] (aggregate.py:249-250, 323-336):
+                # the sum over every row, the count over the non-null ones
                 v = columns[cid]
                 vals.append(v if v.dtype in (torch.float32, torch.float64) else v.to(torch.int64))
                 ops.append('sum')
-                vals.append(torch.ones(n, dtype=torch.int64, device=h.device))
+                vals.append((v != NULL).to(torch.int64))
                 ops.append('sum')
                 post.append(('avg', len(vals) - 2))
             else:
@@ -158,6 +169,11 @@ class KeyedPass1:
             if op == 'avg':
                 agg_vals.append(torch.stack([red[j].to(torch.float64),
                                              red[j + 1].to(torch.float64)], dim=1))
+            elif op == 'max':
+                # MAX folds into a zeroed partial (a scatter_reduce into zeros
+                # that includes them, operator_utils.py:365-369), so a group
+                # whose values are all negative has the partial 0
+                agg_vals.append(torch.clamp_min(red[j], 0))
             else:
                 agg_vals.append(red[j])
         buckets = None
