@@ -968,12 +968,14 @@ __global__ void k_region_starts(unsigned long long* __restrict__ cursor,
   }
 }
 
+constexpr long long P2_SKIP = LLONG_MIN;  // a bin past its region: not written
+
 template <int BINS>
 struct P2Smem {
   P2Row sr[P2TILE];
   int cnt[BINS];           // rows of a bin in the tile, then zero again
   int lofs[BINS];          // a bin's first place in the tile
-  long long gpos[BINS];    // the bin's claimed first place in the output, -1: skip
+  long long gpos[BINS];    // the bin's output place minus its tile place, or P2_SKIP
   int wsum[P2T / 32];
 };
 
@@ -1128,10 +1130,12 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
       pre += q < w ? x : 0;
       total += x;
     }
+    int lofs[BPT];
     {
       int run = pre + incl - s2;
 #pragma unroll
       for (int j = 0; j < BPT; ++j) {
+        lofs[j] = run;
         S.lofs[bt + j] = run;
         run += cb[j];
       }
@@ -1148,14 +1152,16 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
       const int e = S.lofs[slot[q] & (BINS - 1)] + (slot[q] >> LOGBINS);
       S.sr[e] = P2Row{k[q], (long long)v[q]};
     }
+    // per bin, its output place minus its first place in the tile (a row at
+    // tile place e goes to e + that), or the skip mark
 #pragma unroll
     for (int j = 0; j < BPT; ++j) {
-      long long g = gp[j];
-      if (a.cap > 0 && cb[j] && g + cb[j] > (base + bt + j + 1) * a.cap) {
+      long long d = gp[j] - lofs[j];
+      if (a.cap > 0 && cb[j] && gp[j] + cb[j] > (base + bt + j + 1) * a.cap) {
         *a.ovf = 1;  // past the region: none of the bin's rows are written
-        g = -1;
+        d = P2_SKIP;
       }
-      S.gpos[bt + j] = g;
+      S.gpos[bt + j] = d;
     }
     __syncthreads();
     if (tile + gridDim.x < ntiles) {
@@ -1166,9 +1172,9 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
       const P2Row r = S.sr[e];
       const int b = MODE == 0 ? (a.logB2 ? (int)(((uint64_t)r.k >> (64 - a.logS)) & (nb2 - 1)) : 0)
                               : bucket_of_hash((uint64_t)r.k, a.logS);
-      const long long g = S.gpos[b];
-      if (g < 0) continue;
-      const long long pos = g + (e - S.lofs[b]);
+      const long long d = S.gpos[b];
+      if (d == P2_SKIP) continue;
+      const long long pos = d + e;
       if (AOS) {
         a.rec_out[pos] = r;
       } else {
@@ -1176,7 +1182,9 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
         a.val_out[pos] = (int)r.v;
       }
     }
-    __syncthreads();
+    // no barrier here: the next tile's ranking touches only the counts
+    // (zeroed before this tile's second barrier), and its first barrier
+    // waits for every thread's write-out before the staging is reused
   }
 }
 
