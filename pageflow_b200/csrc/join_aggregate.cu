@@ -1015,13 +1015,9 @@ struct P2Args {
 // partition (tstart), the bins are the partition's 2^logB2 sub-buckets; the
 // build side reads and writes (hash, group) columns, the probe side records.
 // RI rows a thread a tile.
-// VEC (first pass, every source column aligned): a thread takes its rows in
-// pairs of neighbours and loads each column's pair with one 16-byte load
-// (8-byte for the groups).
-template <int MODE, bool AOS, int BINS, int RI = P2I, bool VEC = false>
+template <int MODE, bool AOS, int BINS, int RI = P2I>
 __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
   using V = typename std::conditional<AOS, long long, int>::type;
-  static_assert(!VEC || (MODE != 0 && RI % 2 == 0), "paired loads: first pass, even rows");
   constexpr int BPT = BINS / P2T;
   constexpr int TILE = P2T * RI;
   constexpr int LOGBINS = BINS == 4096 ? 12 : BINS == 2048 ? 11 : 10;
@@ -1066,43 +1062,7 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
   // MODE 2 with a discount: the raw price in v and the discount in dv until
   // the tile's turn comes, so the prefetch never waits for its loads
   long long dv[MODE == 2 ? RI : 1];
-  // row q of this thread in the tile from lo
-  auto row_of = [&](long long lo, int q) -> long long {
-    return VEC ? lo + (long long)(q >> 1) * (2 * P2T) + 2 * tid + (q & 1)
-               : lo + (long long)q * P2T + tid;
-  };
   auto load = [&](long long lo, long long hi) {
-    if (VEC) {
-#pragma unroll
-      for (int pq = 0; pq < RI / 2; ++pq) {
-        const long long i = row_of(lo, 2 * pq);
-        if (i + 1 < hi) {
-          const longlong2 kk = stream_ld(reinterpret_cast<const longlong2*>(a.key + i));
-          k[2 * pq] = kk.x;
-          k[2 * pq + 1] = kk.y;
-          if (MODE == 2) {
-            const longlong2 pp =
-                stream_ld(reinterpret_cast<const longlong2*>(reinterpret_cast<const long long*>(a.val) + i));
-            v[2 * pq] = (V)pp.x;
-            v[2 * pq + 1] = (V)pp.y;
-            if (a.disc) {
-              const longlong2 dd = stream_ld(reinterpret_cast<const longlong2*>(a.disc + i));
-              dv[2 * pq] = dd.x;
-              dv[2 * pq + 1] = dd.y;
-            }
-          } else {
-            const int2 gg = stream_ld(reinterpret_cast<const int2*>(reinterpret_cast<const int*>(a.val) + i));
-            v[2 * pq] = (V)gg.x;
-            v[2 * pq + 1] = (V)gg.y;
-          }
-        } else if (i < hi) {
-          k[2 * pq] = stream_ld(a.key + i);
-          v[2 * pq] = stream_ld(reinterpret_cast<const V*>(a.val) + i);
-          if (MODE == 2 && a.disc) dv[2 * pq] = stream_ld(a.disc + i);
-        }
-      }
-      return;
-    }
 #pragma unroll
     for (int q = 0; q < RI; ++q) {
       const long long i = lo + q * P2T + tid;
@@ -1140,7 +1100,7 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
 #pragma unroll
     for (int q = 0; q < RI; ++q) {
       slot[q] = -1;
-      if (row_of(lo, q) < hi) {
+      if (lo + q * P2T + tid < hi) {
         const int b = MODE == 0 ? (a.logB2 ? (int)(((uint64_t)k[q] >> (64 - a.logS)) & (nb2 - 1)) : 0)
                                 : bucket_of_hash((uint64_t)k[q], a.logS);
         slot[q] = (atomicAdd(&S.cnt[b], 1) << LOGBINS) | b;
@@ -2003,12 +1963,12 @@ int count_buckets(const int64_t* build_key, long long n_build, const int64_t* pr
 
 // Launch shape of a tile scatter: opt in to its shared memory, then one
 // block a tile up to the resident blocks of every SM.
-template <int MODE, bool AOS, int BINS, int RI, bool VEC = false>
+template <int MODE, bool AOS, int BINS, int RI>
 int p2_launch(const P2Args& a, long long ntiles, size_t extra_smem, const char* name,
               cudaStream_t st) {
   if (ntiles <= 0) return ok();
   const size_t sm = sizeof(P2Smem<BINS>) + extra_smem;
-  auto kern = k_p2_scatter<MODE, AOS, BINS, RI, VEC>;
+  auto kern = k_p2_scatter<MODE, AOS, BINS, RI>;
   if (int rc = opt_in_smem((const void*)kern, sm)) return rc;
   int per_sm = 0;
   PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, P2T, sm));
@@ -2052,23 +2012,12 @@ int first_pass(const int64_t* build_key, const int32_t* build_group, long long n
   p.rec_out = l.prec;
   constexpr int tb = P2TILE, tp = P2T * P2RI2;
   const long long nbt = (n_build + tb - 1) / tb, npt = (n_probe + tp - 1) / tp;
-  // paired 16-byte loads where the caller's columns allow them
-  const bool vb = aligned16(build_key) && ((uintptr_t)build_group & 7) == 0;
-  const bool vp = aligned16(probe_fk) && aligned16(probe_price) &&
-                  (!probe_disc || aligned16(probe_disc));
-  int rc;
   if (B <= P2BINS) {
-    rc = vb ? p2_launch<1, false, P2BINS, P2I, true>(b, nbt, 0, "k_fscatter_build", st)
-            : p2_launch<1, false, P2BINS, P2I>(b, nbt, 0, "k_fscatter_build", st);
-    if (rc) return rc;
-    return vp ? p2_launch<2, true, P2BINS, P2RI2, true>(p, npt, 0, "k_fscatter_probe", st)
-              : p2_launch<2, true, P2BINS, P2RI2>(p, npt, 0, "k_fscatter_probe", st);
+    if (int rc = p2_launch<1, false, P2BINS, P2I>(b, nbt, 0, "k_fscatter_build", st)) return rc;
+    return p2_launch<2, true, P2BINS, P2RI2>(p, npt, 0, "k_fscatter_probe", st);
   }
-  rc = vb ? p2_launch<1, false, P1BINS, P2I, true>(b, nbt, 0, "k_fscatter_build", st)
-          : p2_launch<1, false, P1BINS, P2I>(b, nbt, 0, "k_fscatter_build", st);
-  if (rc) return rc;
-  return vp ? p2_launch<2, true, P1BINS, P2RI2, true>(p, npt, 0, "k_fscatter_probe", st)
-            : p2_launch<2, true, P1BINS, P2RI2>(p, npt, 0, "k_fscatter_probe", st);
+  if (int rc = p2_launch<1, false, P1BINS, P2I>(b, nbt, 0, "k_fscatter_build", st)) return rc;
+  return p2_launch<2, true, P1BINS, P2RI2>(p, npt, 0, "k_fscatter_probe", st);
 }
 
 // The second pass of one side into sub-partitions.  counted: per-segment
