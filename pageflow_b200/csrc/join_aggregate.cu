@@ -349,16 +349,16 @@ __global__ void __launch_bounds__(TT) k_fscatter_tma(const long long* __restrict
   using V = typename std::conditional<PROBE, long long, int>::type;
   constexpr int TSUB = TSub<PROBE>::rows;
   constexpr int TROWS = TSUB / TT;
-  extern __shared__ __align__(128) unsigned char smem[];
+  extern __shared__ __align__(128) unsigned char tsmem[];
   const TmaSmem<PROBE> L(B, nbuf);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + L.bar);
-  unsigned long long* skey = reinterpret_cast<unsigned long long*>(smem + L.stage_key);
-  V* sval = reinterpret_cast<V*>(smem + L.stage_val);
-  unsigned short* sbk = reinterpret_cast<unsigned short*>(smem + L.sbk);
-  long long* base = reinterpret_cast<long long*>(smem + L.base);
-  int* cnt = reinterpret_cast<int*>(smem + L.cnt);
-  int* tstart = reinterpret_cast<int*>(smem + L.tstart);
-  int* wsum = reinterpret_cast<int*>(smem + L.wsum);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tsmem + L.bar);
+  unsigned long long* skey = reinterpret_cast<unsigned long long*>(tsmem + L.stage_key);
+  V* sval = reinterpret_cast<V*>(tsmem + L.stage_val);
+  unsigned short* sbk = reinterpret_cast<unsigned short*>(tsmem + L.sbk);
+  long long* base = reinterpret_cast<long long*>(tsmem + L.base);
+  int* cnt = reinterpret_cast<int*>(tsmem + L.cnt);
+  int* tstart = reinterpret_cast<int*>(tsmem + L.tstart);
+  int* wsum = reinterpret_cast<int*>(tsmem + L.wsum);
 
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const long long lo = (long long)blockIdx.x * chunk;
@@ -381,7 +381,7 @@ __global__ void __launch_bounds__(TT) k_fscatter_tma(const long long* __restrict
     for (int c = 0; c < ncols; ++c) {
       const unsigned nb = (unsigned)(tma_rows(c, rows) * es[c]);
       if (nb)
-        bulk_g2s(smem + L.in + b * L.in_stride + colofs[c],
+        bulk_g2s(tsmem + L.in + b * L.in_stride + colofs[c],
                  reinterpret_cast<const char*>(src[c]) + sb * es[c], nb, &bar[b]);
     }
   };
@@ -415,7 +415,7 @@ __global__ void __launch_bounds__(TT) k_fscatter_tma(const long long* __restrict
       __syncthreads();
       return;
     }
-    const unsigned char* ib = smem + L.in + b_ * L.in_stride;
+    const unsigned char* ib = tsmem + L.in + b_ * L.in_stride;
     const unsigned long long* ik = reinterpret_cast<const unsigned long long*>(ib + colofs[0]);
     const V* iv = reinterpret_cast<const V*>(ib + colofs[1]);
     const long long* id = reinterpret_cast<const long long*>(ib + colofs[2]);
@@ -590,44 +590,17 @@ __device__ __forceinline__ void build_row(const RoundArgs& a, const uint2* reg, 
   ++overflow;
 }
 
-// Probe one row: its slots from the first (multiply-shift) one on until a
-// free slot (no match) or its key; a match adds the row's value and 1 into its
-// group's (sum, count) pair, both words in one 16-byte cell of the slab.
-__device__ __forceinline__ void probe_row(const RoundArgs& a, const uint2* reg, long long i,
-                                          unsigned long long& matched) {
-  const unsigned long long key = (unsigned long long)a.pfk[i];
-  const uint64_t h = mix64(key);
-  const uint2 r = region_of(a, reg, h);
-  if (r.y == 0) return;
-  unsigned pos = first_slot(h, a.logB, r.y);
-  ulonglong2 sl = ld_slot(a.table + r.x + pos);
-  const long long val = a.pval[i];
-  for (unsigned probes = 1;; ++probes) {
-    if ((uint32_t)(sl.y >> 32) != a.tag) return;  // a free slot: no match
-    if (sl.x == key) {
-      const uint32_t g = (uint32_t)sl.y;
-      if (g != 0xffffffffu) {
-        atomicAdd(&a.slab[2 * (unsigned long long)g], (unsigned long long)val);
-        atomicAdd(&a.slab[2 * (unsigned long long)g + 1], 1ULL);
-      }
-      ++matched;
-      return;
-    }
-    if (probes >= r.y) return;
-    if (++pos == r.y) pos = 0;
-    sl = ld_slot(a.table + r.x + pos);
-  }
-}
-
 // cp.async (16 or 8 bytes, global -> shared, not through registers).
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src)
                : "memory");
 }
+#if !PF_STREAM_HINTS
 __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src)
                : "memory");
 }
+#endif
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
 }
@@ -805,6 +778,12 @@ __global__ void __launch_bounds__(PT2, PF_PROBE_MINB) k_fround(RoundArgs pa, Rou
 #ifndef PF_P2_MINB
 #define PF_P2_MINB 1
 #endif
+#ifndef PF_P2_WU
+#define PF_P2_WU 1
+#endif
+#ifndef PF_P2_SPRE
+#define PF_P2_SPRE 0
+#endif
 constexpr int P2T = PF_P2T;
 constexpr int P2I = PF_P2I;
 constexpr int P2TILE = P2T * P2I;  // rows a tile, at most
@@ -820,12 +799,15 @@ constexpr int P2MAXLOG = 10;       // sub-buckets a partition splits into, log2,
 constexpr int P2BINS = 1 << P2MAXLOG;
 constexpr int P1BINS = FB_MAX;     // the first pass's buckets, at most
 static_assert(P2BINS % P2T == 0 && P1BINS % P2T == 0, "whole bins a thread in the tile scan");
-// Three 384-thread blocks a SM, each with a 3072-slot table (63 KB of shared
-// memory: hash, two-word sum, count; no group offsets), measured against two
-// 512-thread blocks with 4096-slot tables and stored offsets: 4.72 vs 5.43 ms
-// for the 150M x 600M join (more independent blocks overlap the phases).
+// Three 512-thread blocks a SM, each with a 3072-slot table (63 KB of shared
+// memory: hash, two-word sum, count; no group offsets).  Measured on the
+// 150M x 600M join: three 384-thread blocks 4.59 ms, three 512-thread blocks
+// 4.38 (the kernel waits on shared-memory latency: more warps hide more of
+// it), two 512-thread blocks with 4096-slot tables and stored offsets 5.43,
+// two 384-thread blocks 7.19, four 384-thread blocks with 2560-slot tables
+// 4.58, two 1024-thread blocks 5.17.
 #ifndef PF_SJT
-#define PF_SJT 384
+#define PF_SJT 512
 #endif
 #ifndef PF_SJ_MINB
 #define PF_SJ_MINB 3
@@ -1146,12 +1128,22 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
 #pragma unroll
     for (int j = 0; j < BPT; ++j)
       gp[j] = cb[j] ? (long long)atomicAdd(&a.cursor[base + bt + j], (unsigned long long)cb[j]) : 0;
+#if PF_P2_SPRE
+    // every row's tile place first (the loads overlap), then the stores
+#pragma unroll
+    for (int q = 0; q < RI; ++q)
+      if (slot[q] >= 0) slot[q] = S.lofs[slot[q] & (BINS - 1)] + (slot[q] >> LOGBINS);
+#pragma unroll
+    for (int q = 0; q < RI; ++q)
+      if (slot[q] >= 0) S.sr[slot[q]] = P2Row{k[q], (long long)v[q]};
+#else
 #pragma unroll
     for (int q = 0; q < RI; ++q) {
       if (slot[q] < 0) continue;
       const int e = S.lofs[slot[q] & (BINS - 1)] + (slot[q] >> LOGBINS);
       S.sr[e] = P2Row{k[q], (long long)v[q]};
     }
+#endif
     // per bin, its output place minus its first place in the tile (a row at
     // tile place e goes to e + that), or the skip mark
 #pragma unroll
@@ -1168,6 +1160,38 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
       locate(tile + gridDim.x, lo, hi, base);
       load(lo, hi);
     }
+#if PF_P2_WU > 1
+    // PF_P2_WU staged rows a thread at a time: their loads, then their bins'
+    // places, then their stores
+    for (int e0 = tid; e0 < total; e0 += P2T * PF_P2_WU) {
+      P2Row r[PF_P2_WU];
+      long long d[PF_P2_WU];
+#pragma unroll
+      for (int u = 0; u < PF_P2_WU; ++u)
+        if (e0 + u * P2T < total) r[u] = S.sr[e0 + u * P2T];
+#pragma unroll
+      for (int u = 0; u < PF_P2_WU; ++u) {
+        d[u] = P2_SKIP;
+        if (e0 + u * P2T < total) {
+          const int b = MODE == 0
+                            ? (a.logB2 ? (int)(((uint64_t)r[u].k >> (64 - a.logS)) & (nb2 - 1)) : 0)
+                            : bucket_of_hash((uint64_t)r[u].k, a.logS);
+          d[u] = S.gpos[b];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < PF_P2_WU; ++u) {
+        if (d[u] == P2_SKIP) continue;
+        const long long pos = d[u] + e0 + u * P2T;
+        if (AOS) {
+          a.rec_out[pos] = r[u];
+        } else {
+          a.key_out[pos] = r[u].k;
+          a.val_out[pos] = (int)r[u].v;
+        }
+      }
+    }
+#else
     for (int e = tid; e < total; e += P2T) {
       const P2Row r = S.sr[e];
       const int b = MODE == 0 ? (a.logB2 ? (int)(((uint64_t)r.k >> (64 - a.logS)) & (nb2 - 1)) : 0)
@@ -1182,6 +1206,7 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
         a.val_out[pos] = (int)r.v;
       }
     }
+#endif
     // no barrier here: the next tile's ranking touches only the counts
     // (zeroed before this tile's second barrier), and its first barrier
     // waits for every thread's write-out before the staging is reused
@@ -1333,11 +1358,17 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
 #endif
       // build: each build row a slot of its own (all of a thread's rows
       // loaded first)
+      // (and their groups, held until the flush: measured 0.18 ms less than
+      // reading them again there)
       long long bk[SJ_BU];
+      int bg[SJ_BU];
 #pragma unroll
       for (int u = 0; u < SJ_BU; ++u) {
         const int j = u * SJT + tid;
-        if (j < nb) bk[u] = stream_ld(a.bkey + c0 + j);
+        if (j < nb) {
+          bk[u] = stream_ld(a.bkey + c0 + j);
+          bg[u] = stream_ld(a.bgrp + c0 + j);
+        }
       }
 #pragma unroll
       for (int u = 0; u < SJ_BU; ++u) {
@@ -1394,13 +1425,16 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
       }
 #endif
       __syncthreads();
-      // flush every build row that matched (its group read again, from L2),
-      // and empty its slot
-      for (int j = tid; j < nb; j += SJT) {
+      // flush every build row that matched (the thread's own build rows,
+      // their groups in registers), and empty its slot
+#pragma unroll
+      for (int u = 0; u < SJ_BU; ++u) {
+        const int j = u * SJT + tid;
+        if (j >= nb) continue;
         const unsigned t = S.slot_of[j];
         if (t == 0xffff) continue;
         const unsigned c = S.cnt[t];
-        const long long g = (long long)a.bgrp[c0 + j] - a.group_min;
+        const long long g = (long long)bg[u] - a.group_min;
         const bool gok = g >= 0 && g < a.n_groups;
         bad_group += !gok;
         if (c && gok) {
