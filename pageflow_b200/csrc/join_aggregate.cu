@@ -778,11 +778,14 @@ __global__ void __launch_bounds__(PT2, PF_PROBE_MINB) k_fround(RoundArgs pa, Rou
 #ifndef PF_P2_MINB
 #define PF_P2_MINB 1
 #endif
-#ifndef PF_P2_WU
-#define PF_P2_WU 1
+// Staged rows a thread writes out at a time: two for the build side's
+// columns (measured 0.99 -> 0.95 ms for 150M rows), one for the probe side's
+// records (two spill there: 5.68 -> 5.96 ms for the second pass)
+#ifndef PF_P2_WU_SOA
+#define PF_P2_WU_SOA 2
 #endif
-#ifndef PF_P2_SPRE
-#define PF_P2_SPRE 0
+#ifndef PF_P2_WU_AOS
+#define PF_P2_WU_AOS 1
 #endif
 constexpr int P2T = PF_P2T;
 constexpr int P2I = PF_P2I;
@@ -1002,6 +1005,7 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
   using V = typename std::conditional<AOS, long long, int>::type;
   constexpr int BPT = BINS / P2T;
   constexpr int TILE = P2T * RI;
+  constexpr int WU = AOS ? PF_P2_WU_AOS : PF_P2_WU_SOA;
   constexpr int LOGBINS = BINS == 4096 ? 12 : BINS == 2048 ? 11 : 10;
   static_assert(BINS == (1 << LOGBINS) && TILE <= P2TILE, "bins and tile");
   extern __shared__ __align__(16) unsigned char p2_smem[];
@@ -1128,7 +1132,6 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
 #pragma unroll
     for (int j = 0; j < BPT; ++j)
       gp[j] = cb[j] ? (long long)atomicAdd(&a.cursor[base + bt + j], (unsigned long long)cb[j]) : 0;
-#if PF_P2_SPRE
     // every row's tile place first (the loads overlap), then the stores
 #pragma unroll
     for (int q = 0; q < RI; ++q)
@@ -1136,14 +1139,6 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
 #pragma unroll
     for (int q = 0; q < RI; ++q)
       if (slot[q] >= 0) S.sr[slot[q]] = P2Row{k[q], (long long)v[q]};
-#else
-#pragma unroll
-    for (int q = 0; q < RI; ++q) {
-      if (slot[q] < 0) continue;
-      const int e = S.lofs[slot[q] & (BINS - 1)] + (slot[q] >> LOGBINS);
-      S.sr[e] = P2Row{k[q], (long long)v[q]};
-    }
-#endif
     // per bin, its output place minus its first place in the tile (a row at
     // tile place e goes to e + that), or the skip mark
 #pragma unroll
@@ -1160,17 +1155,16 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
       locate(tile + gridDim.x, lo, hi, base);
       load(lo, hi);
     }
-#if PF_P2_WU > 1
-    // PF_P2_WU staged rows a thread at a time: their loads, then their bins'
+    // WU staged rows a thread at a time: their loads, then their bins'
     // places, then their stores
-    for (int e0 = tid; e0 < total; e0 += P2T * PF_P2_WU) {
-      P2Row r[PF_P2_WU];
-      long long d[PF_P2_WU];
+    for (int e0 = tid; e0 < total; e0 += P2T * WU) {
+      P2Row r[WU];
+      long long d[WU];
 #pragma unroll
-      for (int u = 0; u < PF_P2_WU; ++u)
+      for (int u = 0; u < WU; ++u)
         if (e0 + u * P2T < total) r[u] = S.sr[e0 + u * P2T];
 #pragma unroll
-      for (int u = 0; u < PF_P2_WU; ++u) {
+      for (int u = 0; u < WU; ++u) {
         d[u] = P2_SKIP;
         if (e0 + u * P2T < total) {
           const int b = MODE == 0
@@ -1180,7 +1174,7 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
         }
       }
 #pragma unroll
-      for (int u = 0; u < PF_P2_WU; ++u) {
+      for (int u = 0; u < WU; ++u) {
         if (d[u] == P2_SKIP) continue;
         const long long pos = d[u] + e0 + u * P2T;
         if (AOS) {
@@ -1191,22 +1185,6 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
         }
       }
     }
-#else
-    for (int e = tid; e < total; e += P2T) {
-      const P2Row r = S.sr[e];
-      const int b = MODE == 0 ? (a.logB2 ? (int)(((uint64_t)r.k >> (64 - a.logS)) & (nb2 - 1)) : 0)
-                              : bucket_of_hash((uint64_t)r.k, a.logS);
-      const long long d = S.gpos[b];
-      if (d == P2_SKIP) continue;
-      const long long pos = d + e;
-      if (AOS) {
-        a.rec_out[pos] = r;
-      } else {
-        a.key_out[pos] = r.k;
-        a.val_out[pos] = (int)r.v;
-      }
-    }
-#endif
     // no barrier here: the next tile's ranking touches only the counts
     // (zeroed before this tile's second barrier), and its first barrier
     // waits for every thread's write-out before the staging is reused
@@ -1233,8 +1211,8 @@ struct SJArgs {
 // A cell's 64-bit sum in shared memory as two 32-bit words, each in an array
 // of its own (a warp's random cells then spread over all 32 banks), added with
 // 32-bit atomics: the low word's add returns its old value, which shows the
-// carry into the high word (measured against one 64-bit shared add: 0.6 ms
-// less on the 150M x 600M join).
+// carry into the high word (measured against one 64-bit shared add: 4.39
+// against 5.08 ms for the 150M x 600M join).
 struct SJSmem {
   long long key[SJ_TS];
   unsigned sum_lo[SJ_TS];
