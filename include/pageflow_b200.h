@@ -267,12 +267,14 @@ int pf_slab_finish(const uint8_t* occupied, int64_t key_min, int64_t capacity, i
  *
  * The default (shared-memory) path counts no rows before it scatters: each
  * bucket of the first radix pass, and each sub-bucket of the second, owns a
- * region sized for its expected rows plus seven standard deviations, and a
+ * region sized for its expected rows plus seven standard deviations (eight
+ * times the mean's variance on the probe side, whose keys repeat), and a
  * pass whose region would overflow (skewed keys) is run again after counting
- * its rows exactly.  Waits for the first pass's bucket ends (they plan the
- * second pass) and, unless the second pass was counted, for its overflow
- * word at the end; with PF_JOIN_PATH=rounds it waits once, for the bucket
- * counts that plan the rounds, and the rest stays queued.
+ * its rows exactly.  The second pass is planned on the device from the first
+ * pass's cursors, so the call waits once, at the end, for both passes'
+ * overflow words (and again only when one overflowed); with
+ * PF_JOIN_PATH=rounds it waits once, for the bucket counts that plan the
+ * rounds, and the rest stays queued.
  */
 size_t pf_join_aggregate_workspace(int64_t n_build, int64_t n_probe, int B, int64_t n_groups);
 int pf_join_aggregate(const int64_t* build_key, const int32_t* build_group, int64_t n_build,

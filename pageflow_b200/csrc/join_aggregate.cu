@@ -789,13 +789,20 @@ __global__ void __launch_bounds__(PT2, PF_PROBE_MINB) k_fround(RoundArgs pa, Rou
 #endif
 constexpr int P2T = PF_P2T;
 constexpr int P2I = PF_P2I;
-constexpr int P2TILE = P2T * P2I;  // rows a tile, at most
+constexpr int P2TILE = P2T * P2I;  // rows a tile (the build side's passes)
+// The probe side's second pass: rows a thread (its records leave shared
+// memory by bulk copies, so no thread holds rows through a write-out; on
+// 600M probe rows 9 rows a thread measured 0.08 ms less than 8, and 10 spill)
+#ifndef PF_P2I_AOS
+#define PF_P2I_AOS 9
+#endif
+constexpr int P2I_AOS = PF_P2I_AOS;
 // The first pass's probe side carries three input columns a row into its
-// registers: 6 rows a thread (6144-row tiles) keep it within 64 registers
-// without spilling (measured against 8 rows, which spilled: 5.50 vs 5.86 ms
-// on 600M probe rows).
+// registers: 7 rows a thread (7168-row tiles) keep it within 64 registers
+// without spilling (on 600M probe rows: 7 rows 4.85 ms, 6 rows 4.93, 8 rows
+// spill and take longer).
 #ifndef PF_P2_RI2
-#define PF_P2_RI2 6
+#define PF_P2_RI2 7
 #endif
 constexpr int P2RI2 = PF_P2_RI2;
 constexpr int P2MAXLOG = 10;       // sub-buckets a partition splits into, log2, at most
@@ -953,11 +960,64 @@ __global__ void k_region_starts(unsigned long long* __restrict__ cursor,
   }
 }
 
+// After a first pass into regions, on the device (no host wait): per side
+// and partition its start (p * cap) and rows (the cursor's advance, at most
+// cap: a region that overflowed is cut at its end, and the overflow word
+// makes the host run the pass again counted), into pstart ([2B] starts, then
+// [2B] rows), and each partition's first second-pass tile into ts_b / ts_p
+// ([B + 1], the last entry the side's tiles).  One block.
+__global__ void __launch_bounds__(1024) k_pass1_plan(const unsigned long long* __restrict__ cur1,
+                                                     int B, long long cap_b, long long cap_p,
+                                                     long long tile_b, long long tile_p,
+                                                     long long* __restrict__ pstart,
+                                                     int* __restrict__ ts_b,
+                                                     int* __restrict__ ts_p) {
+  __shared__ long long wsum[32];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int per = (B + 1023) / 1024;  // partitions a thread, consecutive
+  for (int side = 0; side < 2; ++side) {
+    const long long cap = side ? cap_p : cap_b, tile = side ? tile_p : tile_b;
+    int* ts = side ? ts_p : ts_b;
+    long long mine = 0;
+    for (int j = 0; j < per; ++j) {
+      const int p = tid * per + j;
+      if (p >= B) break;
+      const long long start = (long long)p * cap;
+      const long long rows = min((long long)cur1[(size_t)side * B + p] - start, cap);
+      pstart[(size_t)side * B + p] = start;
+      pstart[2 * (size_t)B + (size_t)side * B + p] = rows;
+      mine += (rows + tile - 1) / tile;
+    }
+    long long incl = mine;
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long y = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) wsum[w] = incl;
+    __syncthreads();
+    long long pre = 0, total = 0;
+    for (int q = 0; q < 32; ++q) {
+      pre += q < w ? wsum[q] : 0;
+      total += wsum[q];
+    }
+    long long run = pre + incl - mine;
+    for (int j = 0; j < per; ++j) {
+      const int p = tid * per + j;
+      if (p >= B) break;
+      ts[p] = (int)run;
+      const long long rows = pstart[2 * (size_t)B + (size_t)side * B + p];
+      run += (rows + tile - 1) / tile;
+    }
+    if (tid == 0) ts[B] = (int)total;
+    __syncthreads();  // wsum is reused by the other side
+  }
+}
+
 constexpr long long P2_SKIP = LLONG_MIN;  // a bin past its region: not written
 
-template <int BINS>
+template <int BINS, int TILE>
 struct P2Smem {
-  P2Row sr[P2TILE];
+  P2Row sr[TILE];
   int cnt[BINS];           // rows of a bin in the tile, then zero again
   int lofs[BINS];          // a bin's first place in the tile
   long long gpos[BINS];    // the bin's output place minus its tile place, or P2_SKIP
@@ -991,7 +1051,11 @@ struct P2Args {
 // (travelling while the tile is staged in shared memory in bin order), then
 // the write-out with consecutive threads on consecutive places (runs of about
 // P2TILE / 2^logB2 rows).  The next tile's rows are loaded before the
-// write-out.  Order inside a bin is not kept.
+// write-out.  Order inside a bin is not kept.  BULK (16-byte records, a
+// 16-byte aligned output): each bin's run leaves shared memory as one TMA
+// bulk copy issued by the thread that claimed it, instead of thread stores
+// (measured on 600M probe rows: first pass 4.84 -> 4.37 ms, second pass
+// 4.60 -> about 4.0).
 //
 // MODE 1 (first pass, build): rows (key, group) in row order, carried as
 // (mix64(key), group), bins = the B buckets.  MODE 2 (first pass, probe): rows
@@ -1000,17 +1064,19 @@ struct P2Args {
 // partition (tstart), the bins are the partition's 2^logB2 sub-buckets; the
 // build side reads and writes (hash, group) columns, the probe side records.
 // RI rows a thread a tile.
-template <int MODE, bool AOS, int BINS, int RI = P2I>
+template <int MODE, bool AOS, int BINS, int RI, bool BULK>
 __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
   using V = typename std::conditional<AOS, long long, int>::type;
   constexpr int BPT = BINS / P2T;
   constexpr int TILE = P2T * RI;
   constexpr int WU = AOS ? PF_P2_WU_AOS : PF_P2_WU_SOA;
   constexpr int LOGBINS = BINS == 4096 ? 12 : BINS == 2048 ? 11 : 10;
-  static_assert(BINS == (1 << LOGBINS) && TILE <= P2TILE, "bins and tile");
+  static_assert(BINS == (1 << LOGBINS), "bins");
+  static_assert(!BULK || AOS, "bulk copies write 16-byte records");
   extern __shared__ __align__(16) unsigned char p2_smem[];
-  P2Smem<BINS>& S = *reinterpret_cast<P2Smem<BINS>*>(p2_smem);
-  int* tps = reinterpret_cast<int*>(p2_smem + sizeof(P2Smem<BINS>));  // MODE 0
+  using Smem = P2Smem<BINS, TILE>;
+  Smem& S = *reinterpret_cast<Smem*>(p2_smem);
+  int* tps = reinterpret_cast<int*>(p2_smem + sizeof(Smem));  // MODE 0
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int nb2 = 1 << a.logB2;
   const int bt = BPT * tid;  // the first of the bins this thread scans
@@ -1092,6 +1158,7 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
         slot[q] = (atomicAdd(&S.cnt[b], 1) << LOGBINS) | b;
       }
     }
+    if (BULK) bulk_wait_read();  // the last tile's copies have read the staging
     __syncthreads();
     int cb[BPT];
     int s2 = 0;
@@ -1150,38 +1217,56 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
       }
       S.gpos[bt + j] = d;
     }
+    if (BULK) fence_proxy_async_smem();  // the staged rows, to the bulk copies
     __syncthreads();
+    const long long base_cur = base;
     if (tile + gridDim.x < ntiles) {
       locate(tile + gridDim.x, lo, hi, base);
       load(lo, hi);
     }
-    // WU staged rows a thread at a time: their loads, then their bins'
-    // places, then their stores
-    for (int e0 = tid; e0 < total; e0 += P2T * WU) {
-      P2Row r[WU];
-      long long d[WU];
+    if constexpr (BULK) {
+      // each bin's staged run to its claimed place with one bulk copy
+      // (records of 16 bytes: both ends 16-byte aligned); the staging is
+      // reused only after every copy of this tile has read it (the wait
+      // before the next tile's first barrier)
+      bool issued = false;
 #pragma unroll
-      for (int u = 0; u < WU; ++u)
-        if (e0 + u * P2T < total) r[u] = S.sr[e0 + u * P2T];
-#pragma unroll
-      for (int u = 0; u < WU; ++u) {
-        d[u] = P2_SKIP;
-        if (e0 + u * P2T < total) {
-          const int b = MODE == 0
-                            ? (a.logB2 ? (int)(((uint64_t)r[u].k >> (64 - a.logS)) & (nb2 - 1)) : 0)
-                            : bucket_of_hash((uint64_t)r[u].k, a.logS);
-          d[u] = S.gpos[b];
-        }
+      for (int j = 0; j < BPT; ++j) {
+        if (!cb[j]) continue;
+        if (a.cap > 0 && gp[j] + cb[j] > (base_cur + bt + j + 1) * a.cap) continue;
+        bulk_s2g(a.rec_out + gp[j], &S.sr[lofs[j]], (unsigned)cb[j] * (unsigned)sizeof(P2Row));
+        issued = true;
       }
+      if (issued) bulk_commit();
+    } else {
+      // WU staged rows a thread at a time: their loads, then their bins'
+      // places, then their stores
+      for (int e0 = tid; e0 < total; e0 += P2T * WU) {
+        P2Row r[WU];
+        long long d[WU];
 #pragma unroll
-      for (int u = 0; u < WU; ++u) {
-        if (d[u] == P2_SKIP) continue;
-        const long long pos = d[u] + e0 + u * P2T;
-        if (AOS) {
-          a.rec_out[pos] = r[u];
-        } else {
-          a.key_out[pos] = r[u].k;
-          a.val_out[pos] = (int)r[u].v;
+        for (int u = 0; u < WU; ++u)
+          if (e0 + u * P2T < total) r[u] = S.sr[e0 + u * P2T];
+#pragma unroll
+        for (int u = 0; u < WU; ++u) {
+          d[u] = P2_SKIP;
+          if (e0 + u * P2T < total) {
+            const int b =
+                MODE == 0 ? (a.logB2 ? (int)(((uint64_t)r[u].k >> (64 - a.logS)) & (nb2 - 1)) : 0)
+                          : bucket_of_hash((uint64_t)r[u].k, a.logS);
+            d[u] = S.gpos[b];
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < WU; ++u) {
+          if (d[u] == P2_SKIP) continue;
+          const long long pos = d[u] + e0 + u * P2T;
+          if (AOS) {
+            a.rec_out[pos] = r[u];
+          } else {
+            a.key_out[pos] = r[u].k;
+            a.val_out[pos] = (int)r[u].v;
+          }
         }
       }
     }
@@ -1189,6 +1274,7 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
     // (zeroed before this tile's second barrier), and its first barrier
     // waits for every thread's write-out before the staging is reused
   }
+  if (BULK) bulk_wait_all();
 }
 
 struct SJArgs {
@@ -1206,6 +1292,7 @@ struct SJArgs {
   unsigned long long* stats;
   unsigned long long* counter;
   const unsigned long long* ovf;   // nonzero: a region overflowed, nothing to join
+  const unsigned long long* ovf1;  // and the first pass's, when its plan was made on the device
 };
 
 // A cell's 64-bit sum in shared memory as two 32-bit words, each in an array
@@ -1283,7 +1370,8 @@ __device__ __forceinline__ void sj_probe(SJSmem& S, long long key, long long val
 __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
   extern __shared__ __align__(16) unsigned char sj_smem[];
   SJSmem& S = *reinterpret_cast<SJSmem*>(sj_smem);
-  if (*a.ovf) return;  // the partitions are incomplete: the host runs the counted passes
+  // the partitions are incomplete: the host runs the counted passes
+  if (*a.ovf || (a.ovf1 && *a.ovf1)) return;
   const int tid = threadIdx.x;
   for (int t = tid; t < SJ_TS; t += SJT) {
     S.key[t] = SJ_EMPTY;
@@ -1490,7 +1578,7 @@ __device__ __forceinline__ unsigned sjf_home(uint64_t h, int logS) {
 __global__ void __launch_bounds__(SJF_T, PF_SJF_MINB) k_sjoin_fp(SJArgs a) {
   extern __shared__ __align__(16) unsigned char sjf_smem[];
   SJFSmem& S = *reinterpret_cast<SJFSmem*>(sjf_smem);
-  if (*a.ovf) return;  // the partitions are incomplete: the host runs the counted passes
+  if (*a.ovf || (a.ovf1 && *a.ovf1)) return;  // the partitions are incomplete: the host runs the counted passes
   const int tid = threadIdx.x;
   for (int t = tid; t < SJF_TS; t += SJF_T) S.slot[t] = 0;
   for (int r = tid; r < SJF_CAP; r += SJF_T) {
@@ -1979,8 +2067,11 @@ template <int MODE, bool AOS, int BINS, int RI>
 int p2_launch(const P2Args& a, long long ntiles, size_t extra_smem, const char* name,
               cudaStream_t st) {
   if (ntiles <= 0) return ok();
-  const size_t sm = sizeof(P2Smem<BINS>) + extra_smem;
-  auto kern = k_p2_scatter<MODE, AOS, BINS, RI>;
+  const size_t sm = sizeof(P2Smem<BINS, P2T * RI>) + extra_smem;
+  // records leave shared memory by bulk copies when the output is 16-byte
+  // aligned (as the workspace carves it), else by thread stores
+  auto kern = AOS && aligned16(a.rec_out) ? k_p2_scatter<MODE, AOS, BINS, RI, AOS>
+                                          : k_p2_scatter<MODE, AOS, BINS, RI, false>;
   if (int rc = opt_in_smem((const void*)kern, sm)) return rc;
   int per_sm = 0;
   PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, P2T, sm));
@@ -2102,17 +2193,22 @@ int second_pass(const JaLayout& l, const P1View& v, int side, bool counted, long
     *beg = l.beg2 + side * l.s_max;
     *end = cur;
   }
-  // tiles partition by partition
-  std::vector<int> ts((size_t)B + 1);
-  long long nt = 0;
-  for (int p = 0; p < B; ++p) {
-    ts[p] = (int)nt;
-    nt += (hcnt[p] + P2TILE - 1) / P2TILE;
+  // tiles partition by partition (hcnt null: already planned on the device,
+  // their number known there only)
+  const long long tile = side ? (long long)P2T * P2I_AOS : (long long)P2TILE;
+  long long nt = LLONG_MAX;
+  if (hcnt) {
+    std::vector<int> ts((size_t)B + 1);
+    nt = 0;
+    for (int p = 0; p < B; ++p) {
+      ts[p] = (int)nt;
+      nt += (hcnt[p] + tile - 1) / tile;
+    }
+    ts[B] = (int)nt;
+    if (nt >= INT_MAX) return fail(PF_EINVAL, "join_aggregate: too many second-pass tiles");
+    PF_CUDA(cudaMemcpyAsync(l.tstart[side], ts.data(), ts.size() * sizeof(int),
+                            cudaMemcpyHostToDevice, st));
   }
-  ts[B] = (int)nt;
-  if (nt >= INT_MAX) return fail(PF_EINVAL, "join_aggregate: too many second-pass tiles");
-  PF_CUDA(cudaMemcpyAsync(l.tstart[side], ts.data(), ts.size() * sizeof(int),
-                          cudaMemcpyHostToDevice, st));
   P2Args a{};
   a.pstart = d_pstart;
   a.pcnt = d_pcnt;
@@ -2127,7 +2223,7 @@ int second_pass(const JaLayout& l, const P1View& v, int side, bool counted, long
   if (side) {
     a.rec = v.prec;
     a.rec_out = l.prec2;
-    return p2_launch<0, true, P2BINS, P2I>(a, nt, extra, "k_p2_scatter", st);
+    return p2_launch<0, true, P2BINS, P2I_AOS>(a, nt, extra, "k_p2_scatter", st);
   }
   a.key = v.bkey;
   a.val = v.bgrp;
@@ -2143,17 +2239,30 @@ int second_pass(const JaLayout& l, const P1View& v, int side, bool counted, long
 // the caller), the slab split.  A side whose regions would not fit its
 // buffer, or every side after an overflow, takes the counted second pass.
 // Keys are mix64 hashes here.
+//
+// dev (the first pass into regions, its plan made on the device by
+// k_pass1_plan; part unused): partitions are taken at their regions' size,
+// the regions the workspace was sized for, and the host waits once, at the
+// end, for both passes' overflow words; *redo is then 1 when the first pass
+// overflowed (nothing was joined: run everything counted), 2 when only the
+// second did (run the second pass counted from the first pass's cursors).
 int join_smem(const JaLayout& l, const P1View& v, const Knobs& kn, int B, int logB,
               const std::vector<long long>& part, long long group_min, long long n_groups,
               int64_t* sum_out, int64_t* count_out, int64_t* stats_out, long long* hstage,
-              cudaStream_t st) {
-  // pageable source: the copy takes the data before it returns
-  PF_CUDA(cudaMemcpyAsync(l.pstart, part.data(), 4 * (size_t)B * sizeof(long long),
-                          cudaMemcpyHostToDevice, st));
-  const long long* hc = part.data() + 2 * (size_t)B;
+              cudaStream_t st, bool dev = false, int* redo = nullptr) {
+  const long long* hc = nullptr;
   long long maxp[2] = {0, 0};
-  for (int side = 0; side < 2; ++side)
-    for (int p = 0; p < B; ++p) maxp[side] = std::max(maxp[side], hc[(size_t)side * B + p]);
+  if (dev) {
+    maxp[0] = l.cap1[0];
+    maxp[1] = l.cap1[1];
+  } else {
+    // pageable source: the copy takes the data before it returns
+    PF_CUDA(cudaMemcpyAsync(l.pstart, part.data(), 4 * (size_t)B * sizeof(long long),
+                            cudaMemcpyHostToDevice, st));
+    hc = part.data() + 2 * (size_t)B;
+    for (int side = 0; side < 2; ++side)
+      for (int p = 0; p < B; ++p) maxp[side] = std::max(maxp[side], hc[(size_t)side * B + p]);
+  }
   int logB2 = 0;
   while ((maxp[0] >> logB2) > kn.target && logB2 < P2MAXLOG &&
          ((long long)B << (logB2 + 1)) <= l.s_max)
@@ -2169,13 +2278,22 @@ int join_smem(const JaLayout& l, const P1View& v, const Knobs& kn, int B, int lo
     cap2[side] = region_rows((double)maxp[side] / (double)(1LL << logB2), region_var(side));
     counted[side] = kn.counted || S * cap2[side] > l.rows2[side];
   }
+  if (dev && (counted[0] || counted[1])) {
+    // the workspace was sized for these regions, so this does not happen:
+    // if it did, the host's plan takes over (after the first pass's word)
+    PF_CUDA(cudaMemcpyAsync(hstage, l.ovf, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                            st));
+    if (int rc = wait_stream(st)) return rc;
+    *redo = hstage[0] ? 1 : 2;
+    return ok();
+  }
   for (int attempt = 0; attempt < 2; ++attempt) {
     PF_CUDA(cudaMemsetAsync(l.ovf + 1, 0, sizeof(unsigned long long), st));
     const unsigned long long *bbeg, *bend, *pbeg, *pend;
     if (int rc = second_pass(l, v, 0, counted[0], cap2[0], B, logB2, logS, hc, l.pstart,
                              l.pstart + 2 * B, &bbeg, &bend, st))
       return rc;
-    if (int rc = second_pass(l, v, 1, counted[1], cap2[1], B, logB2, logS, hc + B,
+    if (int rc = second_pass(l, v, 1, counted[1], cap2[1], B, logB2, logS, hc ? hc + B : nullptr,
                              l.pstart + B, l.pstart + 3 * B, &pbeg, &pend, st))
       return rc;
     SJArgs a{};
@@ -2194,6 +2312,7 @@ int join_smem(const JaLayout& l, const P1View& v, const Knobs& kn, int B, int lo
     a.stats = (unsigned long long*)stats_out;
     a.counter = l.sj_counter;
     a.ovf = l.ovf + 1;
+    a.ovf1 = dev ? l.ovf : nullptr;
     PF_CUDA(cudaMemsetAsync(l.sj_counter, 0, sizeof(unsigned long long), st));
     if (kn.table) {
       const size_t smem = sizeof(SJFSmem);
@@ -2221,6 +2340,13 @@ int join_smem(const JaLayout& l, const P1View& v, const Knobs& kn, int B, int lo
     g_counted_passes = (g_counted_passes & 1) | (counted[0] || counted[1] ? 2 : 0);
     if (counted[0] && counted[1]) return ok();
     // regions: whether one overflowed (then nothing was joined)
+    if (dev) {
+      PF_CUDA(cudaMemcpyAsync(hstage, l.ovf, 2 * sizeof(unsigned long long),
+                              cudaMemcpyDeviceToHost, st));
+      if (int rc = wait_stream(st)) return rc;
+      *redo = hstage[0] ? 1 : hstage[1] ? 2 : 0;
+      return ok();
+    }
     PF_CUDA(cudaMemcpyAsync(hstage, l.ovf + 1, sizeof(unsigned long long),
                             cudaMemcpyDeviceToHost, st));
     if (int rc = wait_stream(st)) return rc;
@@ -2320,18 +2446,40 @@ extern "C" int pf_join_aggregate_ex(const int64_t* build_key, const int32_t* bui
       if (int rc = first_pass(build_key, build_group, n_build, probe_fk, probe_price, probe_disc,
                               scale, n_probe, logB, B, l.cap1, l, st))
         return rc;
-      // the cursors are the buckets' ends
-      PF_CUDA(cudaMemcpyAsync(hc, l.cur1, 2 * B * sizeof(long long), cudaMemcpyDeviceToHost, st));
-      PF_CUDA(cudaMemcpyAsync(hc + 2 * B, l.ovf, sizeof(long long), cudaMemcpyDeviceToHost, st));
-      if (int rc = wait_stream(st)) return rc;
-      counted = hc[2 * B] != 0;
-      if (!counted)
+      // the second pass and the join queued behind it, planned on the
+      // device from the cursors (the buckets' ends); one host wait, at the end
+      {
+        PF_KERNEL("k_pass1_plan", st);
+        k_pass1_plan<<<1, 1024, 0, st>>>(l.cur1, B, l.cap1[0], l.cap1[1], P2TILE,
+                                         (long long)P2T * P2I_AOS, l.pstart, l.tstart[0],
+                                         l.tstart[1]);
+      }
+      PF_LAUNCH("k_pass1_plan");
+      g_counted_passes = 0;
+      int redo = 0;
+      if (int rc = join_smem(l, P1View{l.pkey, l.pgrp, l.prec}, kn, B, logB, part, group_min,
+                             n_groups, sum_out, count_out, stats_out, hc, st, true, &redo))
+        return rc;
+      if (redo == 0) return ok();
+      if (redo == 1) {
+        counted = true;  // the first pass overflowed: nothing was joined
+      } else {
+        // the second pass overflowed: again from the first pass's cursors,
+        // the second pass counted
+        PF_CUDA(cudaMemcpyAsync(hc, l.cur1, 2 * B * sizeof(long long), cudaMemcpyDeviceToHost,
+                                st));
+        if (int rc = wait_stream(st)) return rc;
         for (int side = 0; side < 2; ++side)
           for (int p = 0; p < B; ++p) {
             const size_t i = (size_t)side * B + p;
             part[i] = p * l.cap1[side];
             part[2 * (size_t)B + i] = hc[i] - part[i];
           }
+        Knobs kc = kn;
+        kc.counted = 1;
+        return join_smem(l, P1View{l.pkey, l.pgrp, l.prec}, kc, B, logB, part, group_min,
+                         n_groups, sum_out, count_out, stats_out, hc, st);
+      }
     }
     if (counted) {
       // a bucket overflowed its region (or counting was asked for): count

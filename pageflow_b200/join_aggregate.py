@@ -137,8 +137,8 @@ class JoinAggregate:
 
     def aggregate(self, build_key, build_group, probe_fk, probe_price, probe_disc=None):
         """Queues the join + dense aggregation into ``self.sum`` /
-        ``self.count`` (waits for the first radix pass's bucket ends, and at
-        the end for the second pass's overflow word)."""
+        ``self.count`` (waits once, at the end, for the radix passes'
+        overflow words; again only after an overflow)."""
         for t, n, dt, name in ((build_key, self.n_build, torch.int64, "build_key"),
                                (build_group, self.n_build, torch.int32, "build_group"),
                                (probe_fk, self.n_probe, torch.int64, "probe_fk"),
