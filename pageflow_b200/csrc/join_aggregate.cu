@@ -781,6 +781,19 @@ __global__ void __launch_bounds__(PT2, PF_PROBE_MINB) k_fround(RoundArgs pa, Rou
 // Staged rows a thread writes out at a time: two for the build side's
 // columns (measured 0.99 -> 0.95 ms for 150M rows), one for the probe side's
 // records (two spill there: 5.68 -> 5.96 ms for the second pass)
+// > 0: each tile's thread 0 prefetches into L2 (one TMA bulk prefetch a
+// column) the rows of the tile that many turns ahead, in the passes that have
+// the registers for it (not the build side's second pass, which would spill).
+// Measured on 150M x 600M rows: one turn ahead (the tile whose register loads
+// this one issues before its write-out) takes the first pass's probe side
+// from 4.37 to 4.19 ms and the second pass from 5.09 to 4.98; two turns ahead
+// is slower than none (4.71, 5.16), three slower still.
+#ifndef PF_P2_L2PF
+#define PF_P2_L2PF 1
+#endif
+#ifndef PF_P2_L2PF_ALL
+#define PF_P2_L2PF_ALL 0
+#endif
 #ifndef PF_P2_WU_SOA
 #define PF_P2_WU_SOA 2
 #endif
@@ -1139,6 +1152,23 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
   }
   __syncthreads();
   for (; tile < ntiles; tile += gridDim.x) {
+#if PF_P2_L2PF
+    // the rows of the tile after the next on their way into L2 (the next
+    // one's are in flight into registers)
+    if ((BULK || MODE == 1 || PF_P2_L2PF_ALL) && tid == 0 &&
+        tile + PF_P2_L2PF * (long long)gridDim.x < ntiles) {
+      long long plo, phi, pbase;
+      locate(tile + PF_P2_L2PF * (long long)gridDim.x, plo, phi, pbase);
+      const unsigned long long n = (unsigned long long)(phi - plo);
+      if (MODE == 0 && AOS) {
+        bulk_prefetch_l2(a.rec + plo, n * sizeof(P2Row));
+      } else {
+        bulk_prefetch_l2(a.key + plo, n * sizeof(long long));
+        bulk_prefetch_l2(reinterpret_cast<const V*>(a.val) + plo, n * sizeof(V));
+        if (MODE == 2 && a.disc) bulk_prefetch_l2(a.disc + plo, n * sizeof(long long));
+      }
+    }
+#endif
     if (MODE != 0) {
 #pragma unroll
       for (int q = 0; q < RI; ++q) k[q] = (long long)mix64((uint64_t)k[q]);
@@ -1194,7 +1224,8 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
       }
     }
     __syncthreads();
-    // the claims travel while the tile is placed
+    // the claims travel while the tile is placed (issued right after the
+    // counts instead: no faster)
     long long gp[BPT];
 #pragma unroll
     for (int j = 0; j < BPT; ++j)

@@ -46,6 +46,23 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
       : "memory");
 }
 
+// Asks the TMA engine to bring [p, p + bytes) of global memory into L2 (no
+// destination, nothing to wait for).  Only whole 16-byte units inside the
+// range are named: the start is rounded up and the end down, so nothing
+// outside it is touched; pieces of at most 64 KiB.
+__device__ __forceinline__ void bulk_prefetch_l2(const void* p, unsigned long long bytes) {
+  unsigned long long a = ((unsigned long long)p + 15) & ~15ULL;
+  const unsigned long long e = ((unsigned long long)p + bytes) & ~15ULL;
+  for (; a < e; a += 65536) {
+    const unsigned n = (unsigned)(e - a < 65536 ? e - a : 65536);
+    asm volatile(
+        "{\n .reg .u64 g;\n cvta.to.global.u64 g, %0;\n"
+        " cp.async.bulk.prefetch.L2.global [g], %1;\n}" ::"l"(a),
+        "r"(n)
+        : "memory");
+  }
+}
+
 // dst (global, 16-byte aligned) <- src (shared, 16-byte aligned), bytes a
 // multiple of 16, in this thread's current bulk group.
 __device__ __forceinline__ void bulk_s2g(void* dst, const void* src, unsigned bytes) {
