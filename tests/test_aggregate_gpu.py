@@ -327,6 +327,51 @@ def test_skewed_probe_keys(B, join_path):
         assert _counted_passes() & (1 if B > 1 else 2)
 
 
+def _unmix64_array(h):
+    """The keys whose mix64 hashes are h (numpy uint64), like _unmix64."""
+    k = h.copy()
+    with np.errstate(over="ignore"):
+        k ^= k >> np.uint64(33)
+        k *= np.uint64(pow(0xc4ceb9fe1a85ec53, -1, 1 << 64))
+        k ^= k >> np.uint64(33)
+        k *= np.uint64(pow(0xff51afd7ed558ccd, -1, 1 << 64))
+        k ^= k >> np.uint64(33)
+    return k.view(np.int64)
+
+
+def test_second_pass_overflow_alone_is_run_again_counted(monkeypatch):
+    """Build keys spread exactly evenly over 64 buckets and their 4
+    sub-buckets (keys made from chosen hashes), ten probe rows a key, and one
+    key repeated 3000 times more: its bucket stays inside its first-pass
+    region (31250 + 3000 of 34832 rows) while its sub-bucket passes its
+    second-pass region (7812 + 3000 of 10588), so only the second pass runs
+    again, counted from the first pass's cursors."""
+    monkeypatch.delenv("PF_JOIN_PATH", raising=False)
+    monkeypatch.delenv("PF_COUNTED", raising=False)
+    rng = np.random.default_rng(5)
+    nb, B, G = 200_000, 64, 5_000
+    cell = np.arange(nb, dtype=np.uint64) % np.uint64(B * 4)      # (bucket, sub-bucket)
+    low = rng.integers(0, 1 << 56, nb, dtype=np.uint64)
+    h = (cell << np.uint64(56)) | low
+    h = np.unique(h)
+    assert len(h) == nb
+    bkey_np = _unmix64_array(h)
+    assert np.array_equal(oracle.mix64(bkey_np).view(np.uint64), h)
+    bkey_np = bkey_np[rng.permutation(nb)]
+    bgrp_np = rng.integers(0, G, nb, dtype=np.int32)
+    fk_np = np.concatenate([np.repeat(bkey_np, 10), np.full(3000, bkey_np[7])])
+    fk_np = fk_np[rng.permutation(len(fk_np))]
+    np_ = len(fk_np)
+    price_np = rng.integers(0, 1 << 30, np_, dtype=np.int64)
+    disc_np = rng.integers(0, 11, np_, dtype=np.int64)
+    args = [torch.from_numpy(x).cuda() for x in (bkey_np, bgrp_np, fk_np, price_np, disc_np)]
+    want = _oracle_groups(*args, 0, G)
+    plan = JoinAggregate(nb, np_, 0, G, "cuda", B=B)
+    _assert_groups(plan.run(*args), want)
+    assert plan.read_stats().matched == want[3] == np_
+    assert _counted_passes() == 2
+
+
 def test_uniform_keys_fill_the_regions_without_counting(join_path):
     w = datagen.scaled(datagen.SCALE, 1 / 300)   # 500K x 2M, 5000 groups
     bkey, bgrp = datagen.gen_build(w, "cuda")
