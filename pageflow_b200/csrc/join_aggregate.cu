@@ -791,9 +791,6 @@ __global__ void __launch_bounds__(PT2, PF_PROBE_MINB) k_fround(RoundArgs pa, Rou
 #ifndef PF_P2_L2PF
 #define PF_P2_L2PF 1
 #endif
-#ifndef PF_P2_L2PF_ALL
-#define PF_P2_L2PF_ALL 0
-#endif
 #ifndef PF_P2_WU_SOA
 #define PF_P2_WU_SOA 2
 #endif
@@ -1155,7 +1152,7 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
 #if PF_P2_L2PF
     // the rows of the tile after the next on their way into L2 (the next
     // one's are in flight into registers)
-    if ((BULK || MODE == 1 || PF_P2_L2PF_ALL) && tid == 0 &&
+    if ((BULK || MODE == 1) && tid == 0 &&
         tile + PF_P2_L2PF * (long long)gridDim.x < ntiles) {
       long long plo, phi, pbase;
       locate(tile + PF_P2_L2PF * (long long)gridDim.x, plo, phi, pbase);
