@@ -496,6 +496,23 @@ def run_sharded(args, w, world, rank, local_rank):
                "ms_per_step": ems / args.e2e_steps}
     moved = sum_over_ranks(sum(job.last["received_rows"]) - sum(job.last["kept_rows"]),
                            world, dev)
+    # per rank: the bytes the step must move in HBM (counts, the partition
+    # pass, the exchange's writes of every received or kept row and reads of
+    # every sent one, the second pass and the join, as on one GPU) and over
+    # NVLink (the rows this rank received from its peers, the slowest rank's)
+    nb, npr = w.n_build, w.n_probe
+    recv = [job.last["received_rows"][s] - job.last["kept_rows"][s] for s in range(2)]
+    link_bytes = max_over_ranks(float(recv[0] * 12 + recv[1] * 16), world, dev)
+    hbm_bytes = (8 * (nb + npr) + nb * 24 + npr * 40 + 2 * (nb * 12 + npr * 16)
+                 + nb * 24 + npr * 32 + nb * 12 + npr * 16)
+    peak, peak_src = measured_peak()
+    step_s = ms / args.steps / 1e3
+    roof = {"bound": "hbm", "kernel": "step, per rank (partition, exchange, second pass, join)",
+            "achieved": hbm_bytes / step_s / 1e9, "peak": peak, "unit": "GB/s",
+            "frac": hbm_bytes / step_s / 1e9 / peak, "traffic": None,
+            "bytes_per_launch": float(hbm_bytes), "peak_source": peak_src}
+    nvlink = {"bytes_received_per_rank": link_bytes, "gbs": link_bytes / step_s / 1e9,
+              "peak": 770.0, "peak_source": "measured peer copy, per direction"}
     if rank == 0:
         line = {
             "metric": "join+agg rows/s", "value": value, "unit": "rows/s", "n_gpus": world,
@@ -508,6 +525,7 @@ def run_sharded(args, w, world, rank, local_rank):
                        "l2": "inputs exceed L2; no flush", "groups_out": groups_out,
                        "matched_probe_rows": matched,
                        "rows_moved_per_step": int(moved)},
+            "roofline": roof, "nvlink": nvlink,
             "e2e": e2e, "clocks": clocks, "gpu_launches": launches,
         }
         print(json.dumps(line), flush=True)
