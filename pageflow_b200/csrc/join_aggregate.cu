@@ -802,7 +802,8 @@ constexpr int P2I = PF_P2I;
 constexpr int P2TILE = P2T * P2I;  // rows a tile (the build side's passes)
 // The probe side's second pass: rows a thread (its records leave shared
 // memory by bulk copies, so no thread holds rows through a write-out; on
-// 600M probe rows 9 rows a thread measured 0.08 ms less than 8, and 10 spill)
+// 600M probe rows 9 rows a thread measured 0.08 ms less than 8; 10 and 11
+// spill and take 0.33 and 0.56 ms more)
 #ifndef PF_P2I_AOS
 #define PF_P2I_AOS 9
 #endif
