@@ -5,7 +5,9 @@
  * cudaStream_t (passed as void*), returns an int status (PF_OK or a negative
  * PF_E* code; pf_last_error() gives the message of the calling thread's last
  * failure) and allocates no device memory: scratch comes from a caller-owned
- * device workspace whose size the matching *_workspace() function reports.
+ * device workspace whose size the matching *_workspace() function reports,
+ * starting on a 256-byte boundary (cudaMalloc's and torch's allocations do;
+ * a workspace that does not is refused with PF_ENOSPACE).
  * Outputs are caller-allocated device buffers sized as each function states.
  * A "host_out" argument is caller-owned PINNED host memory (cudaHostAlloc or
  * cudaHostRegister) that a kernel writes through its device alias.

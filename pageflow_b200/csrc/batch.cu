@@ -425,8 +425,10 @@ extern "C" int pf_batch_prepare(const pf_batch_instance* in, int n, void* worksp
   totals(in, n, &ts, &sp, &items);
   size_t used = 0;
   Layout l = layout((char*)workspace, n, ts, sp, items, &used);
-  if (!workspace || used > workspace_bytes)
-    return fail(PF_ENOSPACE, "batch: workspace of %zu bytes, %zu needed", workspace_bytes, used);
+  if (!workspace || used > workspace_bytes || ((uintptr_t)workspace & 255))
+    return fail(PF_ENOSPACE,
+                "batch: workspace of %zu bytes at %p, %zu needed on a 256-byte boundary",
+                workspace_bytes, workspace, used);
   std::vector<Desc> d(n);
   unsigned long long toff = 0, soff = 0;
   long long bi = 0, pi = 0;

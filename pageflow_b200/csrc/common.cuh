@@ -75,7 +75,11 @@ struct Arena {
     used += count * sizeof(T);
     return p;
   }
-  bool fits() const { return used <= cap; }
+  // the caller's workspace starts on a 256-byte boundary (as cudaMalloc and
+  // torch's allocator return): every carved buffer is then aligned for the
+  // 16-byte vector accesses and bulk copies the kernels make
+  bool aligned() const { return ((uintptr_t)base & 255) == 0; }
+  bool fits() const { return aligned() && used <= cap; }
 };
 
 // ---- host side helpers --------------------------------------------------------

@@ -80,6 +80,24 @@ def test_invalid_arguments_fail_before_any_kernel():
     assert rc == _native.PF_EINVAL and "power of two" in L.pf_last_error().decode()
 
 
+def test_workspace_off_a_256_byte_boundary_is_refused_before_any_kernel():
+    """A workspace must start on a 256-byte boundary (the kernels' 16-byte
+    vector accesses and bulk copies rely on it): one that does not is refused
+    with PF_ENOSPACE before any device work, however large it is."""
+    from pageflow_b200 import _native
+    L = _native.lib()
+    need = L.pf_join_aggregate_workspace(10, 10, 4, 5)
+    for base in ((1 << 20) + 8, (1 << 20) + 128):
+        rc = L.pf_join_aggregate(1, 1, 10, 1, 1, None, 100, 10, 4, 0, 5, 1, 1, 1, base,
+                                 need + 4096, None)
+        assert rc == _native.PF_ENOSPACE, rc
+        assert "workspace" in L.pf_last_error().decode()
+    need = L.pf_join_unique_hash_workspace(10, 10)
+    rc = L.pf_join_unique_hash(1, None, 10, 1, None, 10, 1, 1, 1, 1, (1 << 20) + 16, need + 4096,
+                               None)
+    assert rc == _native.PF_ENOSPACE
+
+
 def test_partition_count_rule_is_the_references():
     from pageflow_b200 import partitions
     g = load("partitions.json")
