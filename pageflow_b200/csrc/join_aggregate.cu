@@ -2100,10 +2100,10 @@ int p2_launch(const P2Args& a, long long ntiles, size_t extra_smem, const char* 
               cudaStream_t st) {
   if (ntiles <= 0) return ok();
   const size_t sm = sizeof(P2Smem<BINS, P2T * RI>) + extra_smem;
-  // records leave shared memory by bulk copies when the output is 16-byte
-  // aligned (as the workspace carves it), else by thread stores
-  auto kern = AOS && aligned16(a.rec_out) ? k_p2_scatter<MODE, AOS, BINS, RI, AOS>
-                                          : k_p2_scatter<MODE, AOS, BINS, RI, false>;
+  // records leave shared memory by bulk copies (the workspace starts on a
+  // 256-byte boundary, so every record output is 16-byte aligned), columns by
+  // thread stores
+  auto kern = k_p2_scatter<MODE, AOS, BINS, RI, AOS>;
   if (int rc = opt_in_smem((const void*)kern, sm)) return rc;
   int per_sm = 0;
   PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, P2T, sm));
