@@ -1,6 +1,6 @@
 """The drop-in as the reference's operators see it (CPU; needs a checkout of
-the reference, named by $PAGEFLOW_REFERENCE or found at the build container's
-usual place, and skips without one).
+the reference, named by $PAGEFLOW_REFERENCE or found as a `reference`
+directory beside this repository, and skips without one).
 
 After ``pageflow_b200.install_as_tqplib()``, the reference's unchanged
 ``operators/partition_sort.py``, ``operators/join_core.py`` and
@@ -20,7 +20,7 @@ from pathlib import Path
 import pytest
 
 REPO = Path(__file__).resolve().parents[1]
-REF = Path(os.environ.get("PAGEFLOW_REFERENCE", "/root/reference"))
+REF = Path(os.environ.get("PAGEFLOW_REFERENCE", str(REPO.parent / "reference")))
 
 pytestmark = pytest.mark.skipif(not (REF / "operators" / "partition_sort.py").exists(),
                                 reason="no reference checkout")
