@@ -172,6 +172,60 @@ class JoinAggregate:
         self.aggregate(build_key, build_group, probe_fk, probe_price, probe_disc)
         return self.finish()
 
+    def run_stream(self, batches):
+        """Joins a sequence of host-resident batches of this plan's shape,
+        each a tuple (build_key, build_group, probe_fk, probe_price,
+        probe_disc or None) of pinned host tensors, and yields each batch's
+        occupied groups as host tensors (keys, sums, counts).  A batch's
+        columns cross to the device on a copy stream while the batch before
+        it is joined, into one of two sets of device buffers (a set is
+        refilled only after the join that read it), so the host link and
+        the GPU work overlap; every batch still crosses the link whole."""
+        dev = self.device
+        compute = torch.cuda.current_stream(dev)
+        copy = torch.cuda.Stream(dev)
+        copy.wait_stream(compute)
+        sets, ready, free = [None, None], [None, None], [None, None]
+
+        def stage(slot, batch):
+            if sets[slot] is None:
+                sets[slot] = [None] * len(batch)
+            for i, h in enumerate(batch):
+                if h is not None and sets[slot][i] is None:
+                    sets[slot][i] = torch.empty(h.shape, dtype=h.dtype, device=dev)
+            with torch.cuda.stream(copy):
+                if free[slot] is not None:
+                    copy.wait_event(free[slot])
+                for d, h in zip(sets[slot], batch):
+                    if h is not None:
+                        d.copy_(h, non_blocking=True)
+                        d.record_stream(copy)   # not reused while the copy may run
+                ready[slot] = torch.cuda.Event()
+                ready[slot].record(copy)
+
+        it = iter(batches)
+        nxt = next(it, None)
+        if nxt is None:
+            return
+        slot = 0
+        stage(slot, nxt)
+        while nxt is not None:
+            cur, nxt = nxt, next(it, None)
+            if nxt is not None:
+                stage(slot ^ 1, nxt)        # crosses the link while this one joins
+            compute.wait_event(ready[slot])
+            dev_in = [d if h is not None else None for d, h in zip(sets[slot], cur)]
+            keys, sums, counts = self.run(*dev_in)
+            out = tuple(torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+                        for t in (keys, sums, counts))
+            for h, d in zip(out, (keys, sums, counts)):
+                h.copy_(d, non_blocking=True)
+            free[slot] = torch.cuda.Event()
+            free[slot].record(compute)
+            free[slot].synchronize()
+            yield out
+            slot ^= 1
+
     def read_stats(self) -> JoinAggregateStats:
         s = self.stats.tolist()
         return JoinAggregateStats(matched=s[0], bad_groups=s[2], overflow=s[3],

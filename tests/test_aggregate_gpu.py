@@ -372,6 +372,28 @@ def test_second_pass_overflow_alone_is_run_again_counted(monkeypatch):
     assert _counted_passes() == 2
 
 
+def test_host_batches_streamed_equal_one_call_each():
+    """run_stream over pinned host batches (each crossing the link while the
+    one before it joins, into alternating device buffers) gives every batch
+    the groups that one call on its device copy gives."""
+    w = datagen.scaled(datagen.SCALE, 1 / 500)
+    bkey, bgrp = datagen.gen_build(w, "cuda")
+    fk, price, disc = datagen.gen_probe(w, "cuda")
+    plan = JoinAggregate(w.n_build, w.n_probe, 0, w.n_groups, "cuda", B=64)
+    batches, want = [], []
+    for shift in (0, 7, 1000):
+        cols = (bkey, bgrp, fk, price + shift, (disc + shift) % 11 if shift else None)
+        keys, sums, counts = plan.run(*cols)
+        want.append((keys.cpu(), sums.cpu(), counts.cpu()))
+        batches.append(tuple(None if c is None else c.cpu().pin_memory() for c in cols))
+    got = list(plan.run_stream(batches + batches[:1]))
+    assert len(got) == 4
+    for g, wnt in zip(got, want + want[:1]):
+        for a, b in zip(g, wnt):
+            assert torch.equal(a, b)
+    assert not torch.equal(got[0][1], got[1][1])
+
+
 def test_uniform_keys_fill_the_regions_without_counting(join_path):
     w = datagen.scaled(datagen.SCALE, 1 / 300)   # 500K x 2M, 5000 groups
     bkey, bgrp = datagen.gen_build(w, "cuda")
