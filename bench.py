@@ -52,7 +52,7 @@ def parse_args(argv=None):
                     help="one join sharded over the ranks (each holds a slice of both sides; "
                          "buckets move to their owners; the default for N > 1) or independent "
                          "replicas (the default for N = 1)")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain-form", action="store_true",
