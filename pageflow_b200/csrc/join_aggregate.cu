@@ -1407,7 +1407,7 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
     S.cnt[t] = 0;
   }
   unsigned matched = 0;  // rows a thread matched (below 2^32: at most 2^40 / SJT)
-  unsigned long long bad_group = 0;
+  unsigned bad_group = 0;  // below 2^32: a thread flushes at most 2^40 / SJT rows
   // Thread 0 fetches the next sub-partition and its ranges into the other
   // half of a double-buffered descriptor while the block works on the
   // current one; the barriers of the work make it visible.
@@ -1558,7 +1558,7 @@ __global__ void __launch_bounds__(SJT, PF_SJ_MINB) k_sjoin(SJArgs a) {
   unsigned long long m = matched;
   for (int o = 16; o; o >>= 1) m += __shfl_xor_sync(FULL, m, o);
   if ((tid & 31) == 0 && m) atomicAdd(&a.stats[0], m);
-  if (bad_group) atomicAdd(&a.stats[2], bad_group);
+  if (bad_group) atomicAdd(&a.stats[2], (unsigned long long)bad_group);
 }
 
 // ---- the join with a fingerprinted slot table ----------------------------------
