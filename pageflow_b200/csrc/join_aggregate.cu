@@ -1054,6 +1054,11 @@ struct P2Args {
   long long* key_out;       // SoA outputs (build side)
   int* val_out;
   P2Row* rec_out;           // AoS output (probe side)
+  // MODE 0 planned on the device: the first pass's overflow word; when it is
+  // raised the partitions are cut short, so the probe side's pass does
+  // nothing (the host runs everything again counted; the build side's pass,
+  // a fifth of the work, runs regardless: the check would cost it registers)
+  const unsigned long long* skip;
 };
 
 // Rows to their bin's run, tile by tile (so the blocks at work at one time
@@ -1098,7 +1103,7 @@ __global__ void __launch_bounds__(P2T, PF_P2_MINB) k_p2_scatter(P2Args a) {
   if (MODE == 0) {
     for (int p = tid; p <= a.B; p += P2T) tps[p] = a.tstart[p];
     __syncthreads();
-    ntiles = tps[a.B];
+    ntiles = AOS && a.skip && *a.skip ? 0 : tps[a.B];
   } else {
     ntiles = (a.n + TILE - 1) / TILE;
   }
@@ -2248,6 +2253,7 @@ int second_pass(const JaLayout& l, const P1View& v, int side, bool counted, long
   a.cursor = cur;
   a.cap = counted ? 0 : cap2;
   a.ovf = l.ovf + 1;
+  a.skip = hcnt ? nullptr : l.ovf;
   const size_t extra = ((size_t)B + 1) * sizeof(int);
   if (side) {
     a.rec = v.prec;
