@@ -13,9 +13,13 @@ Knobs (pf_join_knobs plus the fan-out):
   table     the shared-memory join's table: 8-byte hash slots or 4-byte
             fingerprinted slots
   sub_rows  build rows a sub-partition aims at (1365 or 682)
+  counted   1: both radix passes count their rows first, instead of
+            scattering into regions sized from the expected counts (which a
+            skewed input overflows, paying for a pass it then runs again)
 
 The search is coordinate-wise in that order (B with the default table and
-sub_rows, then the table at the best B, then sub_rows), each candidate run
+sub_rows, then the table at the best B, then sub_rows, then counted), each
+candidate run
 once to warm up and then timed over ``reps`` runs; ties keep the earlier
 candidate, so the same timings always give the same choice.  A shape class
 is the rounded-up log2 of the build rows, probe rows and groups, with the
@@ -34,6 +38,7 @@ from typing import Callable, Dict, List, Optional
 DEFAULT_SUB_ROWS = 1365
 SUB_ROWS = (1365, 682)
 TABLES = (0, 1)
+COUNTED = (0, 1)
 B_MAX = 4096
 
 
@@ -42,9 +47,11 @@ class Choice:
     B: int
     table: int = 0
     sub_rows: int = DEFAULT_SUB_ROWS
+    counted: int = 0
 
     def label(self) -> str:
-        return f"B={self.B},table={self.table},sub_rows={self.sub_rows}"
+        s = f"B={self.B},table={self.table},sub_rows={self.sub_rows}"
+        return s + ",counted=1" if self.counted else s
 
 
 @dataclass
@@ -95,6 +102,7 @@ def search(seed_b: int, time_of: Callable[[Choice], float]) -> Result:
     cur = best_of([Choice(b) for b in b_candidates(seed_b)])
     cur = best_of([Choice(cur.B, t, cur.sub_rows) for t in TABLES])
     cur = best_of([Choice(cur.B, cur.table, s) for s in SUB_ROWS])
+    cur = best_of([Choice(cur.B, cur.table, cur.sub_rows, k) for k in COUNTED])
     return Result(cur, times)
 
 
@@ -123,7 +131,8 @@ def lookup(key: str, path: Optional[Path] = None) -> Optional[Result]:
     if not entry:
         return None
     c = entry["choice"]
-    return Result(Choice(int(c["B"]), int(c["table"]), int(c["sub_rows"])),
+    return Result(Choice(int(c["B"]), int(c["table"]), int(c["sub_rows"]),
+                         int(c.get("counted", 0))),
                   dict(entry.get("times_ms", {})), cached=True)
 
 

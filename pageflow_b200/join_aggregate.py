@@ -111,7 +111,7 @@ class JoinAggregate:
                             self.n_probe, self.n_groups)
 
         def knobs_of(c):
-            return N.JoinKnobs(path=0, table=c.table, sub_rows=c.sub_rows, counted=0)
+            return N.JoinKnobs(path=0, table=c.table, sub_rows=c.sub_rows, counted=c.counted)
 
         def time_of(c):
             kn = knobs_of(c)

@@ -40,7 +40,7 @@ def test_search_is_coordinate_wise_and_deterministic():
     assert r.choice == T.Choice(512, 1, 1365)
     assert calls == ["B=256,table=0,sub_rows=1365", "B=128,table=0,sub_rows=1365",
                      "B=512,table=0,sub_rows=1365", "B=512,table=1,sub_rows=1365",
-                     "B=512,table=1,sub_rows=682"]
+                     "B=512,table=1,sub_rows=682", "B=512,table=1,sub_rows=1365,counted=1"]
     f2, _ = _timer(times)
     assert T.search(256, f2).choice == r.choice
     assert r.times_ms == {k: times.get(k, 100.0) for k in calls}
@@ -55,7 +55,25 @@ def test_cache_round_trip_skips_the_search(tmp_path):
     again = T.tune("k", 256, f, path)
     assert again.cached and again.choice == first.choice and len(calls) == n
     data = json.loads(path.read_text())
-    assert data["k"]["choice"] == {"B": 128, "table": 0, "sub_rows": 1365}
+    assert data["k"]["choice"] == {"B": 128, "table": 0, "sub_rows": 1365, "counted": 0}
     # another shape class searches on its own and keeps the first entry
     T.tune("k2", 64, _timer({})[0], path)
     assert set(json.loads(path.read_text())) == {"k", "k2"}
+
+
+def test_counting_first_wins_where_the_regions_overflow():
+    """A skewed shape class, where scattering into regions overflows and is
+    run again, picks the counted passes; a cache entry without the counted
+    field reads as regions."""
+    times = {"B=256,table=0,sub_rows=1365": 30.0, "B=256,table=0,sub_rows=1365,counted=1": 21.0}
+    f, calls = _timer(times)
+    r = T.search(256, f)
+    assert r.choice == T.Choice(256, 0, 1365, 1)
+    assert calls[-1] == "B=256,table=0,sub_rows=1365,counted=1"
+
+
+def test_old_cache_entries_read_as_regions(tmp_path):
+    path = tmp_path / "tune.json"
+    path.write_text(json.dumps({"k": {"choice": {"B": 64, "table": 1, "sub_rows": 682}}}))
+    hit = T.lookup("k", path)
+    assert hit.cached and hit.choice == T.Choice(64, 1, 682, 0)
