@@ -301,7 +301,7 @@ def run_ours(args, w, world, rank, local_rank):
     if plan.tuning is not None:
         t = plan.tuning
         tuning = {"choice": {"B": t.choice.B, "table": t.choice.table,
-                             "sub_rows": t.choice.sub_rows},
+                             "sub_rows": t.choice.sub_rows, "counted": t.choice.counted},
                   "cached": t.cached, "candidate_ms": t.times_ms}
     elif plan.knobs is None:
         tuning = {"off": "a PF_* override or an explicit --B fixes the configuration"}
